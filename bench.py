@@ -1,0 +1,353 @@
+"""Benchmark: particle-steps/s of the KDK Barnes-Hut step on one B200.
+
+Workload (default): cold collapse, N = 1,048,576 equal-mass bodies uniform in
+the unit sphere, zero velocities, G = 1, eps = 0.005, theta = 0.5,
+quadrupole, dt = 5e-4, seed 1.  A step is one full KDK step of the whole
+system (tree build + force walk + kick/drift), bodies resident on the device.
+
+The JSON line's `value` is the FP32-mixed step (FP32 interactions with
+compensated accumulation, FP64 kick/drift, moments and diagnostics).  Beside
+it: the plain FP64 GPU step (one thread per body, the reference's step
+structure: two tree builds per step), the force error of both against FP64
+direct summation on 4096 seeded bodies, the walk's FP32-pipe roofline, the
+reference's own OpenMP Step() timed on the host cores, and an end-to-end
+figure through the C ABI with host buffers.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at <=1e-3 median force err: FP32-mixed vs FP64 GPU vs CPU"
+WORKLOAD = dict(name="cold_collapse_uniform_sphere", n=1_048_576, eps=0.005, theta=0.5, dt=5e-4, seed=1)
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FLOPS_PP, FLOPS_PC = 20, 56
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        except OSError:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except OSError:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1])]
+        mx = [num(r[2]) for r in rows if num(r[2])]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        busy = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(PEAKS_FILE))
+    except (OSError, ValueError):
+        return {}
+
+
+def force_error(a, d, idx):
+    num = np.sqrt(sum((a[c][idx] - d[c]) ** 2 for c in ("ax", "ay", "az")))
+    den = np.sqrt(sum(d[c] ** 2 for c in ("ax", "ay", "az")))
+    e = num / den
+    return {"median": float(np.median(e)), "p90": float(np.percentile(e, 90)), "p99": float(np.percentile(e, 99))}
+
+
+def time_cpu_reference(bodies, dt, budget_s, threads=None):
+    """The reference's own Step() (oracle/_ref, OpenMP on the host cores) on the same bodies."""
+    from oracle.oracle import Reference
+    R = Reference()
+    threads = threads or os.cpu_count() or 1
+    R.set_threads(threads)
+    n = bodies["x"].shape[0]
+    steps, t_total = 0, 0.0
+    b = dict(bodies)
+    while steps < 1 or (t_total < budget_s and steps < 50):
+        t0 = time.perf_counter()
+        b = R.step(b, dt, 1)
+        t_total += time.perf_counter() - t0
+        steps += 1
+    return {"value": n * steps / t_total, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+            "sample": f"{steps} Step() call(s) of the reference (src/gravity/step.h) on the full "
+                      f"{n}-body system, OpenMP {threads} threads, {t_total:.1f} s"}
+
+
+def run_reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from next_b200 import ic
+    bodies = ic.uniform_sphere(WORKLOAD["n"], seed=WORKLOAD["seed"])
+    steps = max(1, min(args.steps, 2))
+    from oracle.oracle import Reference
+    R = Reference()
+    threads = os.cpu_count() or 1
+    R.set_threads(threads)
+    b = dict(bodies)
+    for _ in range(min(args.warmup, 1)):
+        b = R.step(b, WORKLOAD["dt"], 1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        b = R.step(b, WORKLOAD["dt"], 1)
+    t = time.perf_counter() - t0
+    value = WORKLOAD["n"] * steps / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD["name"], "n_bodies": WORKLOAD["n"], "theta": WORKLOAD["theta"],
+                   "eps": "adaptive (reference softening law)", "dt": WORKLOAD["dt"], "seed": WORKLOAD["seed"],
+                   "physics": "reference as shipped", "l2": "host run"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                         "sample": f"{steps} timed Step() call(s) on the full system after "
+                                   f"{min(args.warmup, 1)} warm-up; bounded so the run ends in minutes"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, world, local = env_rank()
+    from next_b200 import ic
+    from next_b200.native import Simulation, fp32_peak, load
+    lib = load()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                 timeout=__import__("datetime").timedelta(seconds=120))
+        dist = tdist
+    W = WORKLOAD
+    bodies = ic.uniform_sphere(W["n"], seed=W["seed"])
+    n = W["n"]
+    sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local)
+    sim.upload(bodies)
+    # warm-up (establishes tree/stack capacities and the force cache)
+    for _ in range(args.warmup):
+        sim.step(W["dt"])
+    sim.sync()
+    # force error vs FP64 direct summation at the current positions
+    idx = np.random.default_rng(12345).choice(n, 4096, replace=False)
+    a_mixed = sim.accel()
+    d = sim.direct_accel(idx)
+    err_mixed = force_error(a_mixed, d, idx)
+    diag0 = sim.diagnostics()
+    # ---- timed region: K steps, L2 flushed between steps, CUDA events per stage
+    sim.reset_timers()
+    sim.set_timing(True)
+    launches0 = lib.next_kernel_launches()
+    if dist:
+        dist.barrier()
+    sim.sync()
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            sim.flush_l2()
+            sim.step(W["dt"])
+        sim.sync()
+    if dist:
+        dist.barrier()
+    launches = lib.next_kernel_launches() - launches0   # the L2 flushes are memsets, not kernels
+    sim.set_timing(False)
+    st = sim.stats()
+    if st["device_error"]:
+        raise RuntimeError(f"device error word {st['device_error']} during the timed steps")
+    ms_total = st["ms_step"]
+    if dist:
+        import torch
+        t = torch.tensor([ms_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    clocks = clk.summary()
+    diag1 = sim.diagnostics()
+    e0 = diag0["kinetic"] + diag0["potential"]
+    e1 = diag1["kinetic"] + diag1["potential"]
+    value = world * n * args.steps / (ms_total * 1e-3)
+    walk_ms = st["ms_walk"] / max(1, st["walk_launches"])
+    flops_walk = (FLOPS_PP * st["pp_interactions"] + FLOPS_PC * st["pc_interactions"]) / max(1, st["walk_launches"])
+    peak = fp32_peak(local)
+    achieved = flops_walk / (walk_ms * 1e-3) / 1e12
+    # ---- graph replay throughput of the same step (no per-stage events)
+    sim.sync()
+    import ctypes
+    t0 = time.perf_counter()
+    sim.steps(W["dt"], args.steps)
+    sim.sync()
+    graph_s = time.perf_counter() - t0
+    # ---- plain FP64 GPU step (reference step structure, accurate physics)
+    fp64 = None
+    if rank == 0 and not args.skip_fp64:
+        p = Simulation("accurate", "fp64", theta=W["theta"], eps=W["eps"], leaf_cap=1, reuse_forces=False, device=local)
+        p.upload(bodies)
+        p.step(W["dt"])
+        p.sync()
+        a_plain = p.accel()
+        dp = p.direct_accel(idx)
+        err_plain = force_error(a_plain, dp, idx)
+        p.reset_timers()
+        p.set_timing(True)
+        k64 = max(1, args.fp64_steps)
+        for _ in range(k64):
+            p.flush_l2()
+            p.step(W["dt"])
+        p.sync()
+        s64 = p.stats()
+        p.set_timing(False)
+        fp64 = {"value": n * k64 / (s64["ms_step"] * 1e-3), "steps": k64, "ms_per_step": s64["ms_step"] / k64,
+                "force_error": err_plain, "structure": "one thread per body, leaf_cap 1, two tree builds per step"}
+        p.close()
+    # ---- end to end through the C ABI with pinned host buffers
+    e2e = None
+    if rank == 0 and not args.skip_e2e:
+        import ctypes as C
+        bytes_lane = 8 * n
+        ptrs = [lib.next_host_alloc(bytes_lane) for _ in range(7)]
+        lanes = [np.ctypeslib.as_array(C.cast(p_, C.POINTER(C.c_double)), shape=(n,)) for p_ in ptrs]
+        sim.download({k: lanes[i] for i, k in enumerate(("x", "y", "z", "vx", "vy", "vz"))})
+        lanes[6][:] = bodies["m"]
+        e_steps = max(3, args.steps // 4)
+        sim.sync()
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            sim.upload_arrays(lanes)
+            sim.step(W["dt"])
+            sim.download({k: lanes[i] for i, k in enumerate(("x", "y", "z", "vx", "vy", "vz"))})
+        te = time.perf_counter() - t0
+        e2e = {"value": n * e_steps / te, "unit": "particle-steps/s", "h2d_bytes_per_step": 7 * 8 * n + 4 * 0,
+               "d2h_bytes_per_step": 6 * 8 * n, "steps": e_steps,
+               "path": "next_upload (pinned) + next_step + next_download (pinned) per step, host wall clock"}
+        for p_ in ptrs:
+            lib.next_host_free(p_)
+    # ---- CPU baseline: the reference's own Step() on the host cores
+    cpu = None
+    if rank == 0 and not args.skip_cpu:
+        cpu = time_cpu_reference(bodies, W["dt"], args.cpu_budget)
+    sim.close()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return 0
+    peaks = measured_peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 interactions / f64 state", "data": "synthetic",
+        "config": {"workload": W["name"], "n_bodies": n, "theta": W["theta"], "eps": W["eps"], "dt": W["dt"],
+                   "seed": W["seed"], "physics": "accurate (Plummer eps, full-width theta, corrected quadrupole)",
+                   "precision": "FP32-mixed", "leaf_cap": sim.params.leaf_cap, "group_cap": sim.params.group_cap,
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "flushed between steps (256 MiB write outside the timed events); step working set > L2"},
+        "force_error": {"mixed": err_mixed, "fp64_plain": fp64["force_error"] if fp64 else None,
+                        "versus": "FP64 direct summation, 4096 seeded bodies"},
+        "fp64_gpu": fp64,
+        "speedup_vs_fp64_gpu": (value / world) / fp64["value"] if fp64 else None,
+        "graph_value": n * args.steps / graph_s,
+        "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
+        "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / n,
+        "stage_ms_per_step": {"build": st["ms_build"] / args.steps, "sort": st["ms_sort"] / args.steps,
+                              "walk": st["ms_walk"] / args.steps, "other": st["ms_other"] / args.steps},
+        "energy_drift": abs(e1 - e0) / abs(e0),
+        "roofline": {"bound": "fp32", "kernel": "walk_mixed_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                     "peak_source": "measured live by next_fp32_peak (FFMA chains); MEASURED_PEAKS.json has no FP32 entry",
+                     "flops_per_launch": flops_walk, "ms_per_launch": walk_ms,
+                     "flops_rule": "20 per body-body + 56 per body-cell interaction"},
+        "hbm_peak_gbs": peaks.get("hbm_gbs"),
+        "clocks": clocks,
+        "gpu_launches": int(launches),
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

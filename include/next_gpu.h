@@ -1,0 +1,205 @@
+/*
+ * next_gpu.h -- C ABI of the B200 (sm_100a) gravity library libnext_b200.so.
+ *
+ * The library replaces NEXT's gravity hot path: the per-step tree build and
+ * walk inside Step() (src/gravity/step.h:25-204), the octree and its moments
+ * (src/gravity/octree.h:25-128), the force walk bhAccel (octree.h:133-179),
+ * the softening law (src/dt/softening.h:21-35) and computeAdaptiveDt
+ * (src/dt/adaptive.h:23-52).  The reference has no FFI of its own; its
+ * boundary is the header-only C++ call Step(ParticleSystem&, real dt) made by
+ * src/begrun.cpp:97-98.  These entry points are what that call binds to:
+ * next_b200/host/gravity/step.h re-provides Step() and computeAdaptiveDt()
+ * with the reference's signatures on top of them.
+ *
+ * Conventions
+ *  - Every call returns an int status (NEXT_OK = 0).  next_last_error()
+ *    gives a one-line message for the last failure on a handle.
+ *  - All pointers are HOST pointers with plain sizes; device memory is
+ *    owned by the handle.  Arrays are the reference's SoA lanes
+ *    (src/struct/particle.h:22-31): x y z vx vy vz m as double, type as int.
+ *  - Bodies keep the caller's index order at the boundary: index i in an
+ *    upload is index i in every download / force query.
+ *  - One handle per host thread; calls on a handle are ordered on the
+ *    handle's CUDA stream.  Only the calls that return host data block.
+ */
+#ifndef NEXT_GPU_H
+#define NEXT_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define NEXT_OK 0
+#define NEXT_ERR_INVALID_ARGUMENT 1 /* bad size, NULL array, non-finite input, m < 0 */
+#define NEXT_ERR_CUDA 2             /* a CUDA runtime call failed */
+#define NEXT_ERR_OUT_OF_MEMORY 3
+#define NEXT_ERR_NO_BODIES 4        /* step/force call before any upload */
+#define NEXT_ERR_DEVICE 5           /* a kernel raised its error word (see next_stats.device_error) */
+
+/* bits of the device error word (next_stats.device_error) */
+#define NEXT_DEVERR_TREE_OVERFLOW 0x1   /* node/internal/group capacity exceeded */
+#define NEXT_DEVERR_WALK_STACK 0x2      /* walk stack capacity exceeded */
+#define NEXT_DEVERR_SORT_TIMEOUT 0x4    /* radix-sort look-back wait gave up */
+#define NEXT_DEVERR_LIST_OVERFLOW 0x8   /* interaction-list capacity exceeded */
+#define NEXT_DEVERR_BAD_INDEX 0x10      /* an index check failed (tree, sort or reorder); results invalid */
+
+/* ---- physics and precision modes ------------------------------------- */
+/* NEXT_PHYSICS_REFERENCE: the reference's semantics, reproduced exactly --
+ *   one body per leaf, opening test half_width/dist < theta measured to the
+ *   COM (octree.h:153), adaptive softening (softening.h:21-35, octree.h:145-148),
+ *   the reference's quadrupole (octree.h:114-126, 163-172), G fixed at 1.
+ * NEXT_PHYSICS_ACCURATE: Plummer softening eps, full-width opening test
+ *   |COM - x| >= 2*half_width/theta + |COM - centre|, traceless quadrupole
+ *   with parallel-axis terms and the correct sign, leaf buckets of leaf_cap. */
+#define NEXT_PHYSICS_REFERENCE 0
+#define NEXT_PHYSICS_ACCURATE 1
+
+/* NEXT_PRECISION_FP64: plain FP64 walk, one thread per body, depth-first in
+ *   the reference's child order; two tree builds per step as in step.h.
+ * NEXT_PRECISION_MIXED: FP32 interactions in a warp-per-group walk with
+ *   shared-memory interaction lists and compensated accumulation; FP64 for
+ *   positions, velocities, kick/drift, tree moments and diagnostics.
+ *   Requires NEXT_PHYSICS_ACCURATE. */
+#define NEXT_PRECISION_FP64 0
+#define NEXT_PRECISION_MIXED 1
+
+typedef struct next_params {
+    int physics;        /* NEXT_PHYSICS_* */
+    int precision;      /* NEXT_PRECISION_* */
+    double theta;       /* opening angle (reference: 0.5, step.h:32) */
+    double eps;         /* Plummer softening length (accurate mode) */
+    double G;           /* gravitational constant (reference mode forces 1) */
+    int leaf_cap;       /* bodies per leaf before a cell splits (reference mode forces 1) */
+    int group_cap;      /* bodies per walk group, <= 32 (mixed precision) */
+    int quadrupole;     /* 1: monopole + quadrupole; 0: monopole only (accurate mode) */
+    int reuse_forces;   /* 1: the first half-kick reuses a(x_n) from the previous step */
+    int walk_warps;     /* warps per block of the mixed walk */
+    int walk_stack;     /* per-warp traversal stack entries of the mixed walk */
+    int device;         /* CUDA device ordinal */
+} next_params;
+
+typedef struct next_stats {
+    int64_t n_bodies;
+    int64_t n_systems;
+    int64_t n_nodes;         /* tree nodes of the last build */
+    int64_t n_internal;
+    int64_t n_groups;        /* walk groups of the last build (mixed) */
+    int64_t pp_interactions; /* body-body interactions since next_reset_timers */
+    int64_t pc_interactions; /* body-cell interactions since next_reset_timers */
+    int64_t max_stack;       /* deepest walk stack seen since next_reset_timers (mixed) */
+    int32_t device_error;    /* NEXT_DEVERR_* bits */
+    int32_t steps;           /* steps timed since next_reset_timers */
+    double ms_step;          /* summed device time of timed steps (CUDA events) */
+    double ms_build;         /* ... of which keys + sort + reorder + tree + moments */
+    double ms_walk;          /* ... of which force walk */
+    double ms_sort;          /* ... of which radix sort */
+    double ms_other;         /* ... kick/drift and the rest */
+    int64_t walk_launches;   /* walks timed */
+} next_stats;
+
+typedef struct next_handle next_handle;
+
+/* Fill *p with defaults for a physics/precision pair. */
+int next_params_default(next_params* p, int physics, int precision);
+
+int next_create(const next_params* p, next_handle** out);
+void next_destroy(next_handle* h);
+const char* next_last_error(const next_handle* h);
+const char* next_status_string(int status);
+
+/* Upload one system (replaces src/io/load_particle.hpp:100-116's result
+ * being handed to Step).  type may be NULL (all type 0).  If the positions
+ * and masses equal the ones the handle already holds, forces cached by the
+ * previous step stay valid. */
+int next_upload(next_handle* h, int64_t n, const double* x, const double* y, const double* z,
+                const double* vx, const double* vy, const double* vz, const double* m,
+                const int* type);
+
+/* Upload n_systems independent systems at once: system s owns bodies
+ * offsets[s] .. offsets[s+1]-1 (offsets has n_systems+1 entries).  Each
+ * system gets its own root cube, tree and walk; no force acts between
+ * systems.  Segmented keys carry the system number above the octant digits. */
+int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offsets,
+                        const double* x, const double* y, const double* z,
+                        const double* vx, const double* vy, const double* vz,
+                        const double* m, const int* type);
+
+/* Copy the state back in the caller's order.  Any pointer may be NULL. */
+int next_download(next_handle* h, double* x, double* y, double* z,
+                  double* vx, double* vy, double* vz);
+
+/* One KDK leapfrog step (step.h:111-189): v += a dt/2, x += v dt, forces at
+ * the new positions, v += a dt/2. */
+int next_step(next_handle* h, double dt);
+
+/* nsteps steps of fixed dt; with mixed precision each step is one replay of a
+ * captured CUDA graph. */
+int next_steps(next_handle* h, double dt, int nsteps);
+
+/* Forces at the current positions (the quantity bhAccel accumulates,
+ * octree.h:133), in the caller's order.  pot may be NULL; it is filled only
+ * in accurate mode. */
+int next_accel(next_handle* h, double* ax, double* ay, double* az, double* pot);
+
+/* computeAdaptiveDt (src/dt/adaptive.h:23-52) as a device reduction. */
+int next_adaptive_dt(next_handle* h, double base_dt, double* dt_out);
+
+/* FP64 direct summation with Plummer softening eps (and G) of the handle for
+ * the k bodies idx[0..k) (caller's indices).  pot may be NULL. */
+int next_direct_accel(next_handle* h, int64_t k, const int64_t* idx,
+                      double* ax, double* ay, double* az, double* pot);
+
+/* FP64 diagnostics: out[0] kinetic energy, out[1] potential energy (from the
+ * walk; accurate mode), out[2..4] momentum, out[5..7] angular momentum. */
+int next_diagnostics(next_handle* h, double* out8);
+
+int next_stats_get(next_handle* h, next_stats* s);
+int next_set_timing(next_handle* h, int on);
+int next_reset_timers(next_handle* h);
+int next_sync(next_handle* h);
+
+/* Octant keys (the reference's insertion path, octree.h:49-64, 21 levels of
+ * 3 bits from bit 62 down) of the uploaded bodies in the caller's order, and
+ * the root cube (cx, cy, cz, half-width) of step.h:69-100. */
+int next_debug_keys(next_handle* h, uint64_t* keys, double* cube4);
+
+/* Stable key order of the last build: perm[p] = caller's index of the p-th
+ * body in key order. */
+int next_debug_order(next_handle* h, int64_t* perm);
+
+/* Build the tree at the current positions and export it depth-first
+ * (children in octant order, the order bhAccel visits them) as 16 doubles
+ * per node: level, m, com x y z, half-width, Qxx Qyy Qzz Qxy Qxz Qyz, leaf,
+ * body index (one-body leaf, else -1), 0, body count.  *n_rows = node count. */
+int next_debug_tree(next_handle* h, double* rows, int64_t cap, int64_t* n_rows);
+
+/* Stable LSD radix sort of (key, value) pairs on the device, the sort the
+ * tree build uses: n pairs in, sorted pairs out (host arrays). */
+int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const uint32_t* vals_in,
+                    uint64_t* keys_out, uint32_t* vals_out, int key_bits);
+
+/* Sustained FP32 FMA throughput of the device (TFLOP/s), by a chain-of-FMA
+ * kernel; the denominator of the walk's roofline. */
+int next_fp32_peak(int device, double* tflops, double* sm_mhz_hint);
+
+/* Write a buffer larger than L2 on the handle's stream (untimed helper for
+ * benchmarks that flush L2 between steps). */
+int next_flush_l2(next_handle* h);
+
+/* Page-locked host memory for body arrays, so uploads and downloads run at
+ * full PCIe/C2C bandwidth.  Free with next_host_free. */
+void* next_host_alloc(int64_t bytes);
+void next_host_free(void* p);
+
+/* Kernels this library has launched in this process (graph replays count
+ * every kernel node of the graph). */
+int64_t next_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEXT_GPU_H */

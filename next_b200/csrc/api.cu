@@ -1,0 +1,1046 @@
+// Host runtime and C ABI of libnext_b200.so (see include/next_gpu.h).
+//
+// A handle owns one CUDA stream and all device memory of one simulation:
+// two ping-pong copies of the body SoA (working order = key order of the
+// last build), keys, sort scratch, the tree, and small scalars.  A KDK step
+// (src/gravity/step.h:111-189) is
+//     [forces at x_n]        -- skipped when reuse_forces and still valid
+//     kick + drift           -- v += a dt/2 ; x += v dt
+//     forces at x_{n+1}      -- root cubes, keys, sort, reorder, tree, walk
+//     kick                   -- v += a dt/2
+// A tree/stack capacity overflow raises a device error bit; every later
+// kernel of the step then does nothing but permute bodies, so the host grows
+// the capacity and re-runs only the force phase and the closing kick.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace nb;
+
+#include <atomic>
+
+namespace nb {
+static std::atomic<int64_t> g_launches{0};
+void count_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+int64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace nb
+
+namespace {
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc(reinterpret_cast<void**>(p), sizeof(T) * count);
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+struct BodyBuf {
+    Bodies b{};
+    void alloc_all(int64_t n, cudaError_t& e) {
+        auto A = [&](auto** p, size_t c) { if (e == cudaSuccess) e = dalloc(p, c); };
+        A(&b.x, n); A(&b.y, n); A(&b.z, n); A(&b.vx, n); A(&b.vy, n); A(&b.vz, n); A(&b.m, n);
+        A(&b.type, n); A(&b.id, n);
+    }
+    void free_all() {
+        dfree(b.x); dfree(b.y); dfree(b.z); dfree(b.vx); dfree(b.vy); dfree(b.vz); dfree(b.m);
+        dfree(b.type); dfree(b.id);
+    }
+};
+
+constexpr int kReduceMax = 1024;
+
+}  // namespace
+
+struct next_handle {
+    next_params prm{};
+    Params P{};
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t st = nullptr;
+    std::string last_error;
+
+    // bodies
+    int64_t n = 0, cap_n = 0;
+    int nsys = 0;
+    std::vector<int64_t> offsets_h;
+    Systems sys{};
+    BodyBuf buf[2];
+    int cur = 0;                      // buf[cur] holds the working state
+    double *ax = nullptr, *ay = nullptr, *az = nullptr, *pot = nullptr;
+    uint64_t *keys = nullptr, *keys_alt = nullptr;
+    uint32_t *idx = nullptr, *idx_alt = nullptr;
+    uint32_t* inv = nullptr;
+    int32_t* sysid = nullptr;
+    int64_t* d_offsets = nullptr;
+    double4* cubes = nullptr;
+    uint32_t* sort_scratch = nullptr;
+    size_t sort_words = 0;
+    double* stage = nullptr;          // 7 x n staging lanes (upload) / up to 10 x n (download)
+    int* stype = nullptr;
+    const double** lanes_dev = nullptr;
+
+    // tree
+    Tree t{};
+    void* scan_tmp = nullptr;
+    int64_t scan_tmp_elems = 0;
+
+    // small device scalars
+    int* err = nullptr;
+    unsigned long long* stats = nullptr;   // pp, pc, max stack, spare
+    unsigned int* queue = nullptr;
+    unsigned int* tickets = nullptr;       // 0: cubes, 1: dt, 2: diagnostics
+    double* partial = nullptr;             // kReduceMax * 8
+    double* dts = nullptr;                 // dt, dt/2
+    double* dt_out = nullptr;              // adaptive dt, half
+    double* diag = nullptr;                // 8
+    int* changed = nullptr;
+    float* fma_out = nullptr;
+
+    // pinned host scalars
+    double* h_dts = nullptr;
+    int* h_err = nullptr;
+    int64_t* h_counts = nullptr;           // internal, nodes, groups
+    unsigned long long* h_stats = nullptr;
+
+    // direct summation scratch
+    int64_t* d_targets = nullptr;
+    int64_t* d_targetpos = nullptr;
+    double* d_direct_partial = nullptr;
+    double* d_direct_out = nullptr;
+    int64_t direct_cap = 0;
+    int direct_slice_cap = 0;
+
+    // L2 flush buffer
+    void* flush = nullptr;
+    size_t flush_bytes = 0;
+
+    // state
+    bool have_bodies = false;
+    bool forces_valid = false;
+    bool pot_valid = false;
+    bool sorted_in_alt = false;
+
+    // graphs: one captured KDK step per buffer parity
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int64_t graph_kernels[2] = {0, 0};
+
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::vector<int>> ev_steps;   // per timed step: event indices
+    double acc_step = 0, acc_build = 0, acc_walk = 0, acc_sort = 0, acc_other = 0;
+    int64_t timed_steps = 0, timed_walks = 0;
+
+    Bodies cur_bodies() const {
+        Bodies b = buf[cur].b;
+        b.ax = ax; b.ay = ay; b.az = az; b.pot = pot;
+        return b;
+    }
+};
+
+namespace {
+
+int fail(next_handle* h, int code, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+int cuda_fail(next_handle* h, cudaError_t e, const char* where) {
+    return fail(h, e == cudaErrorMemoryAllocation ? NEXT_ERR_OUT_OF_MEMORY : NEXT_ERR_CUDA,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define NB_TRY(expr, where)                                   \
+    do {                                                      \
+        cudaError_t e__ = (expr);                             \
+        if (e__ != cudaSuccess) return cuda_fail(h, e__, where); \
+    } while (0)
+
+void free_tree(next_handle* h) {
+    Tree& t = h->t;
+    dfree(t.dlev); dfree(t.nint); dfree(t.int_start); dfree(t.int_level); dfree(t.int_bounds);
+    dfree(t.int_packed); dfree(t.int_node); dfree(t.counter); dfree(t.link); dfree(t.parent); dfree(t.level);
+    dfree(t.com); dfree(t.quad64); dfree(t.box); dfree(t.quad32); dfree(t.groups);
+    dfree(h->scan_tmp);
+    t.cap_int = t.cap_node = t.cap_group = 0;
+}
+
+void drop_graphs(next_handle* h) {
+    for (auto& g : h->graph)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+int alloc_tree(next_handle* h, int64_t cap_int) {
+    drop_graphs(h);
+    free_tree(h);
+    Tree& t = h->t;
+    const int64_t n = h->cap_n;
+    t.cap_int = cap_int;
+    t.cap_node = std::min<int64_t>(8 * cap_int, cap_int + n) + h->nsys + 64;
+    t.cap_group = n + h->nsys + 64;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](auto** p, size_t c) { if (e == cudaSuccess) e = dalloc(p, c); };
+    A(&t.dlev, n + 1); A(&t.nint, n + 1);
+    A(&t.int_start, cap_int); A(&t.int_level, cap_int); A(&t.int_bounds, 9 * cap_int);
+    A(&t.int_packed, cap_int + 1); A(&t.int_node, cap_int); A(&t.counter, cap_int);
+    A(&t.link, t.cap_node); A(&t.parent, t.cap_node); A(&t.level, t.cap_node);
+    A(&t.com, t.cap_node); A(&t.quad64, 8 * t.cap_node);
+    if (h->P.physics == NEXT_PHYSICS_ACCURATE) { A(&t.box, t.cap_node); A(&t.quad32, 2 * t.cap_node); }
+    A(&t.groups, t.cap_group);
+    h->scan_tmp_elems = scan_tile_sums_needed(std::max<int64_t>(n + 1, cap_int + 1));
+    int64_t* st64 = nullptr;
+    A(&st64, h->scan_tmp_elems);
+    h->scan_tmp = st64;
+    if (e != cudaSuccess) return cuda_fail(h, e, "tree allocation");
+    NB_TRY(cudaMemsetAsync(t.counter, 0, sizeof(int32_t) * cap_int, h->st), "tree counters");
+    NB_TRY(cudaMemsetAsync(t.link, 0, sizeof(int2) * t.cap_node, h->st), "tree links");
+    return NEXT_OK;
+}
+
+int64_t initial_cap_int(const next_handle* h) {
+    const int leaf = h->P.physics == NEXT_PHYSICS_REFERENCE ? 1 : std::max(1, h->P.leaf_cap);
+    return h->cap_n / leaf + h->cap_n / (4 * leaf) + 1024;
+}
+
+void free_bodies(next_handle* h) {
+    drop_graphs(h);
+    for (auto& b : h->buf) b.free_all();
+    dfree(h->ax); dfree(h->ay); dfree(h->az); dfree(h->pot);
+    dfree(h->keys); dfree(h->keys_alt); dfree(h->idx); dfree(h->idx_alt); dfree(h->inv);
+    dfree(h->sysid); dfree(h->d_offsets); dfree(h->cubes); dfree(h->sort_scratch);
+    dfree(h->stage); dfree(h->stype);
+    if (h->lanes_dev) { cudaFree(h->lanes_dev); h->lanes_dev = nullptr; }
+    free_tree(h);
+    h->cap_n = 0;
+}
+
+int alloc_bodies(next_handle* h, int64_t n) {
+    free_bodies(h);
+    h->cap_n = n;
+    cudaError_t e = cudaSuccess;
+    h->buf[0].alloc_all(n, e);
+    h->buf[1].alloc_all(n, e);
+    auto A = [&](auto** p, size_t c) { if (e == cudaSuccess) e = dalloc(p, c); };
+    A(&h->ax, n); A(&h->ay, n); A(&h->az, n); A(&h->pot, n);
+    A(&h->keys, n); A(&h->keys_alt, n); A(&h->idx, n); A(&h->idx_alt, n); A(&h->inv, n);
+    A(&h->sysid, n); A(&h->d_offsets, h->nsys + 1); A(&h->cubes, h->nsys);
+    h->sort_words = sort_scratch_words(n);
+    A(&h->sort_scratch, h->sort_words);
+    A(&h->stage, 10 * n); A(&h->stype, n);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&h->lanes_dev), sizeof(double*) * 16);
+    if (e != cudaSuccess) return cuda_fail(h, e, "body allocation");
+    return alloc_tree(h, initial_cap_int(h));
+}
+
+bool finite_array(const double* a, int64_t n) {
+    for (int64_t i = 0; i < n; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+
+// ---- the force phase -------------------------------------------------------
+
+int record(next_handle* h, std::vector<int>* evs) {
+    if (!evs) return NEXT_OK;
+    if (h->ev_used >= h->ev_pool.size()) {
+        cudaEvent_t ev;
+        NB_TRY(cudaEventCreate(&ev), "event create");
+        h->ev_pool.push_back(ev);
+    }
+    NB_TRY(cudaEventRecord(h->ev_pool[h->ev_used], h->st), "event record");
+    evs->push_back(static_cast<int>(h->ev_used++));
+    return NEXT_OK;
+}
+
+// Root cubes, keys, sort, reorder, tree, moments (no walk).
+int build(next_handle* h, std::vector<int>* evs) {
+    const int64_t n = h->n;
+    Bodies src = h->cur_bodies();
+    int rc0 = record(h, evs);
+    if (rc0) return rc0;
+    NB_TRY(launch_root_cubes(src, n, h->sys, h->d_offsets, h->partial, kReduceMax, h->tickets + 0, h->st), "root cube");
+    NB_TRY(launch_keys(src, h->sysid, n, h->sys, h->keys, h->idx, h->st), "keys");
+    rc0 = record(h, evs);
+    if (rc0) return rc0;
+    bool in_alt = false;
+    NB_TRY(radix_sort_pairs(h->keys, h->idx, h->keys_alt, h->idx_alt, n, 63, h->sort_scratch, h->err, &in_alt, h->st),
+           "radix sort");
+    h->sorted_in_alt = in_alt;
+    int rc = record(h, evs);
+    if (rc) return rc;
+    const uint64_t* skeys = in_alt ? h->keys_alt : h->keys;
+    const uint32_t* sidx = in_alt ? h->idx_alt : h->idx;
+    const int other = 1 - h->cur;
+    Bodies dst = h->buf[other].b;
+    NB_TRY(launch_gather_bodies(h->buf[h->cur].b, dst, sidx, n, h->inv, h->err, h->st), "reorder");
+    h->cur = other;
+    Bodies bd = h->cur_bodies();
+    NB_TRY(build_tree(skeys, n, bd, h->sysid, h->sys, h->d_offsets, h->P, h->t, h->scan_tmp, h->err, h->st),
+           "tree build");
+    h->forces_valid = false;
+    return record(h, evs);
+}
+
+int walk(next_handle* h, bool potential) {
+    Bodies bd = h->cur_bodies();
+    if (h->prm.precision == NEXT_PRECISION_MIXED) {
+        NB_TRY(launch_walk_mixed(bd, h->n, h->t, h->P, potential, h->prm.walk_warps, h->prm.walk_stack, h->queue, h->stats,
+                                 h->err, h->sm_count, h->st),
+               "mixed walk");
+    } else {
+        NB_TRY(launch_walk_plain(bd, h->sysid, h->n, h->t, h->P, h->nsys > 1, h->stats, h->err, h->st), "plain walk");
+    }
+    return NEXT_OK;
+}
+
+int forces(next_handle* h, bool potential, std::vector<int>* evs) {
+    int rc = build(h, evs);
+    if (rc) return rc;
+    rc = walk(h, potential);
+    if (rc) return rc;
+    h->forces_valid = true;
+    h->pot_valid = potential;
+    return record(h, evs);
+}
+
+int read_device_error(next_handle* h, int* bits) {
+    NB_TRY(cudaMemcpyAsync(h->h_err, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->st), "error word");
+    NB_TRY(cudaMemcpyAsync(h->h_counts, h->t.counts, sizeof(int64_t) * 3, cudaMemcpyDeviceToHost, h->st), "counts");
+    NB_TRY(cudaMemcpyAsync(h->h_stats, h->stats, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, h->st), "stats");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    *bits = *h->h_err;
+    return NEXT_OK;
+}
+
+// Grow what overflowed, clear the error word.  Returns NEXT_OK if the step
+// can be retried.
+int recover(next_handle* h, int bits) {
+    if (bits & (kErrSort | kErrList | kErrIndex))
+        return fail(h, NEXT_ERR_DEVICE, "device error word " + std::to_string(bits) +
+                                            " (sort look-back timeout or failed index check)");
+    if (bits & kErrTree) {
+        const int64_t need = std::max<int64_t>(h->h_counts[0] + h->h_counts[0] / 2 + 1024, 2 * h->t.cap_int);
+        int rc = alloc_tree(h, need);
+        if (rc) return rc;
+    }
+    if (bits & kErrStack) {
+        if (h->prm.walk_stack >= (1 << 14)) return fail(h, NEXT_ERR_DEVICE, "walk stack capacity limit reached");
+        h->prm.walk_stack *= 2;
+        drop_graphs(h);
+    }
+    NB_TRY(cudaMemsetAsync(h->err, 0, sizeof(int), h->st), "error reset");
+    return NEXT_OK;
+}
+
+// Force phase with overflow recovery (synchronous).
+int forces_checked(next_handle* h, bool potential) {
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        int rc = forces(h, potential, nullptr);
+        if (rc) return rc;
+        int bits = 0;
+        rc = read_device_error(h, &bits);
+        if (rc) return rc;
+        if (bits == 0) return NEXT_OK;
+        rc = recover(h, bits);
+        if (rc) return rc;
+    }
+    return fail(h, NEXT_ERR_DEVICE, "force phase kept overflowing");
+}
+
+int set_dt(next_handle* h, double dt) {
+    NB_TRY(launch_set_dt(h->dts, dt, h->st), "dt upload");
+    return NEXT_OK;
+}
+
+// One eager step.  With evs, events bracket the stages for timing.
+int step_once(next_handle* h, bool sync_checked) {
+    const bool reuse = h->prm.reuse_forces && h->forces_valid;
+    std::vector<int> evs;
+    std::vector<int>* E = h->timing ? &evs : nullptr;
+    int rc = record(h, E);
+    if (rc) return rc;
+    if (!reuse) {
+        rc = sync_checked ? forces_checked(h, false) : forces(h, false, nullptr);
+        if (rc) return rc;
+    }
+    Bodies bd = h->cur_bodies();
+    NB_TRY(launch_kick_drift(bd, h->n, h->dts, h->err, h->st), "kick-drift");
+    rc = forces(h, false, E);
+    if (rc) return rc;
+    bd = h->cur_bodies();
+    NB_TRY(launch_kick(bd, h->n, h->dts, h->err, h->st), "kick");
+    rc = record(h, E);
+    if (rc) return rc;
+    if (E) h->ev_steps.push_back(evs);
+    if (!sync_checked) return NEXT_OK;
+    int bits = 0;
+    rc = read_device_error(h, &bits);
+    if (rc) return rc;
+    if (bits == 0) return NEXT_OK;
+    // the kick-drift ran; redo the force phase and the closing kick
+    rc = recover(h, bits);
+    if (rc) return rc;
+    rc = forces_checked(h, false);
+    if (rc) return rc;
+    bd = h->cur_bodies();
+    NB_TRY(launch_kick(bd, h->n, h->dts, h->err, h->st), "kick");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    return NEXT_OK;
+}
+
+// Capture kick-drift + force phase + kick for the current buffer parity.
+int capture_step(next_handle* h) {
+    const int parity = h->cur;
+    if (h->graph[parity]) return NEXT_OK;
+    const bool saved_timing = h->timing;
+    h->timing = false;
+    const int saved_cur = h->cur;
+    cudaGraph_t g = nullptr;
+    const int64_t launches_before = launches_so_far();
+    NB_TRY(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed), "begin capture");
+    int rc = NEXT_OK;
+    Bodies bd = h->cur_bodies();
+    cudaError_t e = launch_kick_drift(bd, h->n, h->dts, h->err, h->st);
+    if (e == cudaSuccess) rc = forces(h, false, nullptr);
+    if (e == cudaSuccess && rc == NEXT_OK) {
+        bd = h->cur_bodies();
+        e = launch_kick(bd, h->n, h->dts, h->err, h->st);
+    }
+    cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
+    const int64_t captured = launches_so_far() - launches_before;
+    count_launches(static_cast<int>(-captured));   // captured, not launched
+    h->graph_kernels[parity] = captured;
+    h->cur = saved_cur;
+    h->timing = saved_timing;
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(h, e, "capture"); }
+    if (e2 != cudaSuccess) return cuda_fail(h, e2, "end capture");
+    e = cudaGraphInstantiate(&h->graph[parity], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
+    return NEXT_OK;
+}
+
+int check_ready(next_handle* h) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (!h->have_bodies) return fail(h, NEXT_ERR_NO_BODIES, "no bodies uploaded");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "set device");
+    return NEXT_OK;
+}
+
+int resolve_timers(next_handle* h) {
+    if (h->ev_steps.empty()) return NEXT_OK;
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    for (const auto& ev : h->ev_steps) {
+        if (ev.size() != 7) continue;
+        auto el = [&](int a, int b) {
+            float v = 0.f;
+            cudaEventElapsedTime(&v, h->ev_pool[ev[a]], h->ev_pool[ev[b]]);
+            return static_cast<double>(v);
+        };
+        const double step = el(0, 6), build = el(1, 4), walkms = el(4, 5), sortms = el(2, 3);
+        h->acc_step += step;
+        h->acc_build += build;
+        h->acc_walk += walkms;
+        h->acc_sort += sortms;
+        h->acc_other += step - build - walkms;
+        h->timed_steps += 1;
+        h->timed_walks += 1;
+    }
+    h->ev_steps.clear();
+    h->ev_used = 0;
+    return NEXT_OK;
+}
+
+// Grow capacities that the last build came close to (before a graph capture).
+int grow_if_tight(next_handle* h) {
+    const int64_t internal = h->h_counts[0], nodes = h->h_counts[1];
+    if (4 * internal > 3 * h->t.cap_int || 4 * nodes > 3 * h->t.cap_node) {
+        int rc = alloc_tree(h, std::max<int64_t>(2 * internal + 1024, h->t.cap_int));
+        if (rc) return rc;
+        h->forces_valid = false;
+    }
+    if (h->prm.precision == NEXT_PRECISION_MIXED && 4 * static_cast<int64_t>(h->h_stats[2]) > 3 * h->prm.walk_stack &&
+        h->prm.walk_stack < (1 << 14)) {
+        h->prm.walk_stack *= 2;
+        drop_graphs(h);
+    }
+    return NEXT_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char* next_status_string(int s) {
+    switch (s) {
+        case NEXT_OK: return "ok";
+        case NEXT_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case NEXT_ERR_CUDA: return "CUDA error";
+        case NEXT_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case NEXT_ERR_NO_BODIES: return "no bodies uploaded";
+        case NEXT_ERR_DEVICE: return "device error";
+        default: return "unknown status";
+    }
+}
+
+const char* next_last_error(const next_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int next_params_default(next_params* p, int physics, int precision) {
+    if (!p) return NEXT_ERR_INVALID_ARGUMENT;
+    std::memset(p, 0, sizeof(*p));
+    p->physics = physics;
+    p->precision = precision;
+    p->theta = 0.5;
+    p->eps = physics == NEXT_PHYSICS_REFERENCE ? 0.0 : 0.01;
+    p->G = 1.0;
+    p->leaf_cap = physics == NEXT_PHYSICS_REFERENCE ? 1 : (precision == NEXT_PRECISION_MIXED ? 16 : 1);
+    p->group_cap = 32;
+    p->quadrupole = 1;
+    p->reuse_forces = precision == NEXT_PRECISION_MIXED ? 1 : 0;
+    p->walk_warps = 4;
+    p->walk_stack = 1024;
+    p->device = 0;
+    return NEXT_OK;
+}
+
+int next_create(const next_params* p, next_handle** out) {
+    if (!p || !out) return NEXT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if ((p->physics != NEXT_PHYSICS_REFERENCE && p->physics != NEXT_PHYSICS_ACCURATE) ||
+        (p->precision != NEXT_PRECISION_FP64 && p->precision != NEXT_PRECISION_MIXED) ||
+        (p->precision == NEXT_PRECISION_MIXED && p->physics != NEXT_PHYSICS_ACCURATE) || !(p->theta > 0.0) ||
+        !(p->eps >= 0.0) || !std::isfinite(p->eps) || !std::isfinite(p->G) || p->leaf_cap < 1 || p->leaf_cap > 64 ||
+        p->group_cap < 1 || p->group_cap > 32 || p->walk_warps < 1 || p->walk_warps > 8 || p->walk_stack < 64 ||
+        p->walk_stack > (1 << 14) ||
+        (p->precision == NEXT_PRECISION_MIXED && p->leaf_cap > p->group_cap))
+        return NEXT_ERR_INVALID_ARGUMENT;
+    next_handle* h = new (std::nothrow) next_handle();
+    if (!h) return NEXT_ERR_OUT_OF_MEMORY;
+    h->prm = *p;
+    h->P.physics = p->physics;
+    h->P.theta = p->theta;
+    h->P.eps = p->physics == NEXT_PHYSICS_REFERENCE ? 0.0 : p->eps;
+    h->P.G = p->physics == NEXT_PHYSICS_REFERENCE ? 1.0 : p->G;
+    h->P.leaf_cap = p->physics == NEXT_PHYSICS_REFERENCE ? 1 : p->leaf_cap;
+    h->P.group_cap = p->group_cap;
+    h->P.quad = p->quadrupole ? 1 : 0;
+    h->device = p->device;
+    auto bail = [&](cudaError_t e, const char* w) {
+        int rc = cuda_fail(h, e, w);
+        next_destroy(h);
+        return rc;
+    };
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return bail(e, "set device");
+    e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->device);
+    if (e != cudaSuccess) return bail(e, "device attribute");
+    e = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(e, "stream");
+    e = sort_prepare();
+    if (e != cudaSuccess) return bail(e, "sort setup");
+    auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
+    A(&h->err, 1); A(&h->stats, 4); A(&h->queue, 1); A(&h->tickets, 4); A(&h->partial, kReduceMax * 8);
+    A(&h->dts, 2); A(&h->dt_out, 2); A(&h->diag, 8); A(&h->changed, 1); A(&h->fma_out, 1);
+    A(&h->t.counts, 4);
+    if (e != cudaSuccess) return bail(e, "scalars");
+    e = cudaMemset(h->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->tickets, 0, sizeof(unsigned int) * 4);
+    if (e == cudaSuccess) e = cudaMemset(h->stats, 0, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess) e = cudaMemset(h->t.counts, 0, sizeof(int64_t) * 4);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_dts), sizeof(double) * 2, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_err), sizeof(int) * 2, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_counts), sizeof(int64_t) * 4, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_stats), sizeof(unsigned long long) * 4, cudaHostAllocDefault);
+    if (e != cudaSuccess) return bail(e, "pinned scalars");
+    *out = h;
+    return NEXT_OK;
+}
+
+void next_destroy(next_handle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->st) cudaStreamSynchronize(h->st);
+    free_bodies(h);
+    dfree(h->err); dfree(h->stats); dfree(h->queue); dfree(h->tickets); dfree(h->partial);
+    dfree(h->dts); dfree(h->dt_out); dfree(h->diag); dfree(h->changed); dfree(h->fma_out); dfree(h->t.counts);
+    dfree(h->d_targets); dfree(h->d_targetpos); dfree(h->d_direct_partial); dfree(h->d_direct_out);
+    if (h->flush) cudaFree(h->flush);
+    for (auto ev : h->ev_pool) cudaEventDestroy(ev);
+    if (h->h_dts) cudaFreeHost(h->h_dts);
+    if (h->h_err) cudaFreeHost(h->h_err);
+    if (h->h_counts) cudaFreeHost(h->h_counts);
+    if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offsets, const double* x, const double* y,
+                        const double* z, const double* vx, const double* vy, const double* vz, const double* m,
+                        const int* type) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (n_systems < 1 || n_systems > (1 << 20) || !offsets)
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "n_systems must be in [1, 2^20] with offsets");
+    if (offsets[0] != 0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "offsets[0] must be 0");
+    for (int64_t s = 0; s < n_systems; ++s)
+        if (offsets[s + 1] < offsets[s]) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "offsets must not decrease");
+    const int64_t n = offsets[n_systems];
+    if (n < 1 || n >= (int64_t(1) << 30))
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "body count must be in [1, 2^30)");
+    if (!x || !y || !z || !vx || !vy || !vz || !m) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "NULL body array");
+    for (const double* a : {x, y, z, vx, vy, vz, m})
+        if (!finite_array(a, n)) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "non-finite body data");
+    for (int64_t i = 0; i < n; ++i)
+        if (m[i] < 0.0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "negative mass");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "set device");
+    const bool same_layout = h->have_bodies && h->n == n && h->nsys == n_systems &&
+                             std::equal(offsets, offsets + n_systems + 1, h->offsets_h.begin());
+    if (!same_layout) {
+        h->have_bodies = false;
+        h->forces_valid = false;
+        h->nsys = static_cast<int>(n_systems);
+        h->offsets_h.assign(offsets, offsets + n_systems + 1);
+        int rc = alloc_bodies(h, n);
+        if (rc) return rc;
+        h->n = n;
+        Systems& S = h->sys;
+        S.n = h->nsys;
+        if (h->nsys == 1) {
+            S.base = 63;
+            S.levels = kMaxLevel;
+        } else {
+            int bits = 0;
+            while ((int64_t(1) << bits) < n_systems) ++bits;
+            S.base = 63 - bits;
+            S.levels = std::min(kMaxLevel, S.base / 3);
+        }
+        S.offsets = h->d_offsets;
+        S.cube = h->cubes;
+        NB_TRY(cudaMemcpyAsync(h->d_offsets, offsets, sizeof(int64_t) * (n_systems + 1), cudaMemcpyHostToDevice, h->st),
+               "offsets");
+        std::vector<int32_t> sid(n);
+        for (int64_t s = 0; s < n_systems; ++s)
+            for (int64_t i = offsets[s]; i < offsets[s + 1]; ++i) sid[i] = static_cast<int32_t>(s);
+        NB_TRY(cudaMemcpyAsync(h->sysid, sid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->st), "system ids");
+        NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    }
+    const double* lanes[7] = {x, y, z, vx, vy, vz, m};
+    for (int c = 0; c < 7; ++c)
+        NB_TRY(cudaMemcpyAsync(h->stage + c * n, lanes[c], sizeof(double) * n, cudaMemcpyHostToDevice, h->st), "upload");
+    if (type) {
+        NB_TRY(cudaMemcpyAsync(h->stype, type, sizeof(int) * n, cudaMemcpyHostToDevice, h->st), "upload types");
+    } else {
+        NB_TRY(cudaMemsetAsync(h->stype, 0, sizeof(int) * n, h->st), "types");
+    }
+    Bodies b = h->cur_bodies();
+    if (same_layout) {
+        NB_TRY(cudaMemsetAsync(h->changed, 0, sizeof(int), h->st), "compare flag");
+        NB_TRY(launch_compare(h->stage, h->stype, b, h->inv, n, h->changed, h->st), "compare");
+        NB_TRY(cudaMemcpyAsync(h->h_err + 1, h->changed, sizeof(int), cudaMemcpyDeviceToHost, h->st), "compare flag");
+        NB_TRY(cudaStreamSynchronize(h->st), "sync");
+        if (h->h_err[1] == 0) {
+            NB_TRY(launch_load_velocities(h->stage, b, h->inv, n, h->st), "velocities");
+            return NEXT_OK;   // same positions: tree order and cached forces stay valid
+        }
+    }
+    NB_TRY(launch_load_all(h->stage, h->stype, b, h->inv, n, h->st), "load");
+    h->forces_valid = false;
+    h->have_bodies = true;
+    return NEXT_OK;
+}
+
+int next_upload(next_handle* h, int64_t n, const double* x, const double* y, const double* z, const double* vx,
+                const double* vy, const double* vz, const double* m, const int* type) {
+    const int64_t offs[2] = {0, n};
+    return next_upload_systems(h, 1, offs, x, y, z, vx, vy, vz, m, type);
+}
+
+int next_download(next_handle* h, double* x, double* y, double* z, double* vx, double* vy, double* vz) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    const Bodies b = h->cur_bodies();
+    const double* src[6] = {b.x, b.y, b.z, b.vx, b.vy, b.vz};
+    double* dst[6] = {x, y, z, vx, vy, vz};
+    const double* lanes[6];
+    double* outs[6];
+    int cnt = 0;
+    for (int c = 0; c < 6; ++c)
+        if (dst[c]) { lanes[cnt] = src[c]; outs[cnt] = dst[c]; ++cnt; }
+    if (cnt == 0) return NEXT_OK;
+    NB_TRY(cudaMemcpyAsync(h->lanes_dev, lanes, sizeof(double*) * cnt, cudaMemcpyHostToDevice, h->st), "lanes");
+    NB_TRY(launch_gather_out(h->lanes_dev, cnt, h->inv, h->n, h->stage, h->st), "gather out");
+    for (int c = 0; c < cnt; ++c)
+        NB_TRY(cudaMemcpyAsync(outs[c], h->stage + c * h->n, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->st),
+               "download");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    return NEXT_OK;
+}
+
+int next_step(next_handle* h, double dt) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!std::isfinite(dt)) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "dt must be finite");
+    rc = set_dt(h, dt);
+    if (rc) return rc;
+    return step_once(h, !h->timing);
+}
+
+int next_steps(next_handle* h, double dt, int nsteps) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!std::isfinite(dt) || nsteps < 0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad dt or step count");
+    rc = set_dt(h, dt);
+    if (rc) return rc;
+    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces && !h->timing;
+    int done = 0;
+    while (done < nsteps) {
+        if (!use_graph || !h->forces_valid) {
+            rc = step_once(h, !h->timing);
+            if (rc) return rc;
+            ++done;
+            continue;
+        }
+        // replay the captured step; buffers alternate, so keep one graph per parity
+        if (!h->graph[h->cur]) {
+            int bits = 0;
+            rc = read_device_error(h, &bits);
+            if (rc) return rc;
+            rc = grow_if_tight(h);
+            if (rc) return rc;
+            if (!h->forces_valid) continue;
+        }
+        rc = capture_step(h);
+        if (rc) return rc;
+        NB_TRY(cudaGraphLaunch(h->graph[h->cur], h->st), "graph launch");
+        count_launches(static_cast<int>(h->graph_kernels[h->cur]));
+        h->cur = 1 - h->cur;
+        ++done;
+        if (done == nsteps || (done & 63) == 0) {
+            int bits = 0;
+            rc = read_device_error(h, &bits);
+            if (rc) return rc;
+            if (bits) return fail(h, NEXT_ERR_DEVICE,
+                                  "device error word " + std::to_string(bits) + " during graph replay; use next_step");
+            rc = grow_if_tight(h);
+            if (rc) return rc;
+        }
+    }
+    h->forces_valid = true;
+    return NEXT_OK;
+}
+
+int next_accel(next_handle* h, double* ax, double* ay, double* az, double* pot) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    const bool want_pot = pot && h->P.physics == NEXT_PHYSICS_ACCURATE;
+    if (!h->forces_valid || (want_pot && !h->pot_valid)) {
+        rc = forces_checked(h, want_pot);
+        if (rc) return rc;
+    }
+    const double* lanes[4] = {h->ax, h->ay, h->az, h->pot};
+    double* outs[4] = {ax, ay, az, pot};
+    const int cnt = want_pot ? 4 : 3;
+    NB_TRY(cudaMemcpyAsync(h->lanes_dev, lanes, sizeof(double*) * cnt, cudaMemcpyHostToDevice, h->st), "lanes");
+    NB_TRY(launch_gather_out(h->lanes_dev, cnt, h->inv, h->n, h->stage, h->st), "gather out");
+    for (int c = 0; c < cnt; ++c)
+        if (outs[c])
+            NB_TRY(cudaMemcpyAsync(outs[c], h->stage + c * h->n, sizeof(double) * h->n, cudaMemcpyDeviceToHost, h->st),
+                   "download");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    if (pot && !want_pot) std::memset(pot, 0, sizeof(double) * h->n);
+    return NEXT_OK;
+}
+
+int next_adaptive_dt(next_handle* h, double base_dt, double* dt_out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!dt_out) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "NULL output");
+    NB_TRY(launch_adaptive_dt(h->cur_bodies(), h->n, base_dt, h->partial, h->tickets + 1, h->dt_out, h->st), "adaptive dt");
+    NB_TRY(cudaMemcpyAsync(h->h_dts, h->dt_out, sizeof(double), cudaMemcpyDeviceToHost, h->st), "dt");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    *dt_out = h->h_dts[0];
+    return NEXT_OK;
+}
+
+int next_direct_accel(next_handle* h, int64_t k, const int64_t* idx, double* ax, double* ay, double* az, double* pot) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (k < 0 || (k > 0 && !idx)) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad sample");
+    for (int64_t t = 0; t < k; ++t)
+        if (idx[t] < 0 || idx[t] >= h->n) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "sample index out of range");
+    if (h->nsys != 1) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "direct summation needs a single system");
+    if (k == 0) return NEXT_OK;
+    const int slices = direct_slices(h->n, k);
+    if (k > h->direct_cap || slices > h->direct_slice_cap) {
+        dfree(h->d_targets); dfree(h->d_targetpos); dfree(h->d_direct_partial); dfree(h->d_direct_out);
+        cudaError_t e = cudaSuccess;
+        auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
+        A(&h->d_targets, k); A(&h->d_targetpos, k); A(&h->d_direct_partial, 4 * k * slices); A(&h->d_direct_out, 4 * k);
+        if (e != cudaSuccess) return cuda_fail(h, e, "direct scratch");
+        h->direct_cap = k;
+        h->direct_slice_cap = slices;
+    }
+    NB_TRY(cudaMemcpyAsync(h->d_targets, idx, sizeof(int64_t) * k, cudaMemcpyHostToDevice, h->st), "sample");
+    NB_TRY(launch_ids_to_positions(h->d_targets, h->inv, k, h->d_targetpos, h->st), "sample map");
+    const double eps = h->P.physics == NEXT_PHYSICS_REFERENCE ? h->prm.eps : h->P.eps;
+    NB_TRY(launch_direct(h->cur_bodies(), h->n, h->d_targetpos, k, eps, h->P.G, h->d_direct_partial, slices,
+                         h->d_direct_out, h->st),
+           "direct sum");
+    std::vector<double> out(4 * k);
+    NB_TRY(cudaMemcpyAsync(out.data(), h->d_direct_out, sizeof(double) * 4 * k, cudaMemcpyDeviceToHost, h->st), "direct out");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    for (int64_t t = 0; t < k; ++t) {
+        if (ax) ax[t] = out[4 * t];
+        if (ay) ay[t] = out[4 * t + 1];
+        if (az) az[t] = out[4 * t + 2];
+        if (pot) pot[t] = out[4 * t + 3];
+    }
+    return NEXT_OK;
+}
+
+int next_diagnostics(next_handle* h, double* out8) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!out8) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "NULL output");
+    const bool acc = h->P.physics == NEXT_PHYSICS_ACCURATE;
+    if (acc && (!h->forces_valid || !h->pot_valid)) {
+        rc = forces_checked(h, true);
+        if (rc) return rc;
+    }
+    NB_TRY(launch_diagnostics(h->cur_bodies(), h->n, acc, h->partial, h->tickets + 2, h->diag, h->st), "diagnostics");
+    NB_TRY(cudaMemcpyAsync(out8, h->diag, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->st), "diagnostics");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    return NEXT_OK;
+}
+
+int next_stats_get(next_handle* h, next_stats* s) {
+    if (!h || !s) return NEXT_ERR_INVALID_ARGUMENT;
+    std::memset(s, 0, sizeof(*s));
+    s->n_bodies = h->n;
+    s->n_systems = h->nsys;
+    if (h->have_bodies) {
+        int bits = 0;
+        int rc = read_device_error(h, &bits);
+        if (rc) return rc;
+        rc = resolve_timers(h);
+        if (rc) return rc;
+        s->device_error = bits;
+        s->n_internal = h->h_counts[0];
+        s->n_nodes = h->h_counts[1];
+        s->n_groups = h->h_counts[2];
+        s->pp_interactions = static_cast<int64_t>(h->h_stats[0]);
+        s->pc_interactions = static_cast<int64_t>(h->h_stats[1]);
+        s->max_stack = static_cast<int64_t>(h->h_stats[2]);
+    }
+    s->steps = static_cast<int32_t>(h->timed_steps);
+    s->ms_step = h->acc_step;
+    s->ms_build = h->acc_build;
+    s->ms_walk = h->acc_walk;
+    s->ms_sort = h->acc_sort;
+    s->ms_other = h->acc_other;
+    s->walk_launches = h->timed_walks;
+    return NEXT_OK;
+}
+
+int next_set_timing(next_handle* h, int on) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    h->timing = on != 0;
+    return NEXT_OK;
+}
+
+int next_reset_timers(next_handle* h) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (h->st) cudaStreamSynchronize(h->st);
+    h->ev_steps.clear();
+    h->ev_used = 0;
+    h->acc_step = h->acc_build = h->acc_walk = h->acc_sort = h->acc_other = 0;
+    h->timed_steps = h->timed_walks = 0;
+    NB_TRY(cudaMemsetAsync(h->stats, 0, sizeof(unsigned long long) * 4, h->st), "stats reset");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    return NEXT_OK;
+}
+
+int next_sync(next_handle* h) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    return NEXT_OK;
+}
+
+int next_debug_keys(next_handle* h, uint64_t* keys, double* cube4) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    Bodies b = h->cur_bodies();
+    NB_TRY(launch_root_cubes(b, h->n, h->sys, h->d_offsets, h->partial, kReduceMax, h->tickets + 0, h->st), "root cube");
+    NB_TRY(launch_keys(b, h->sysid, h->n, h->sys, h->keys, h->idx, h->st), "keys");
+    std::vector<uint64_t> kw(h->n);
+    std::vector<uint32_t> ids(h->n);
+    NB_TRY(cudaMemcpyAsync(kw.data(), h->keys, sizeof(uint64_t) * h->n, cudaMemcpyDeviceToHost, h->st), "keys");
+    NB_TRY(cudaMemcpyAsync(ids.data(), b.id, sizeof(uint32_t) * h->n, cudaMemcpyDeviceToHost, h->st), "ids");
+    if (cube4)
+        NB_TRY(cudaMemcpyAsync(cube4, h->cubes, sizeof(double) * 4, cudaMemcpyDeviceToHost, h->st), "cube");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    if (keys)
+        for (int64_t p = 0; p < h->n; ++p) keys[ids[p]] = kw[p];
+    return NEXT_OK;
+}
+
+int next_debug_order(next_handle* h, int64_t* perm) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (!h->forces_valid) {
+        rc = forces_checked(h, false);
+        if (rc) return rc;
+    }
+    std::vector<uint32_t> ids(h->n);
+    NB_TRY(cudaMemcpyAsync(ids.data(), h->cur_bodies().id, sizeof(uint32_t) * h->n, cudaMemcpyDeviceToHost, h->st), "ids");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    for (int64_t p = 0; p < h->n; ++p) perm[p] = ids[p];
+    return NEXT_OK;
+}
+
+int next_debug_tree(next_handle* h, double* rows, int64_t cap, int64_t* n_rows) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    rc = forces_checked(h, false);
+    if (rc) return rc;
+    const int64_t nn = h->h_counts[1];
+    std::vector<int2> link(nn);
+    std::vector<int8_t> level(nn);
+    std::vector<double4> com(nn);
+    std::vector<double> q64(8 * nn);
+    std::vector<uint32_t> ids(h->n);
+    NB_TRY(cudaMemcpyAsync(link.data(), h->t.link, sizeof(int2) * nn, cudaMemcpyDeviceToHost, h->st), "tree");
+    NB_TRY(cudaMemcpyAsync(level.data(), h->t.level, nn, cudaMemcpyDeviceToHost, h->st), "tree");
+    NB_TRY(cudaMemcpyAsync(com.data(), h->t.com, sizeof(double4) * nn, cudaMemcpyDeviceToHost, h->st), "tree");
+    NB_TRY(cudaMemcpyAsync(q64.data(), h->t.quad64, sizeof(double) * 8 * nn, cudaMemcpyDeviceToHost, h->st), "tree");
+    NB_TRY(cudaMemcpyAsync(ids.data(), h->cur_bodies().id, sizeof(uint32_t) * h->n, cudaMemcpyDeviceToHost, h->st), "ids");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    int64_t count = 0;
+    std::vector<int> stackv;
+    for (int r = h->nsys - 1; r >= 0; --r) stackv.push_back(r);
+    while (!stackv.empty()) {
+        const int nd = stackv.back();
+        stackv.pop_back();
+        if (count < cap && rows) {
+            double* o = rows + 16 * count;
+            const bool leaf = link[nd].y <= 0;
+            const int cnt = leaf ? -link[nd].y : 0;
+            o[0] = level[nd]; o[1] = com[nd].w; o[2] = com[nd].x; o[3] = com[nd].y; o[4] = com[nd].z;
+            o[5] = q64[8 * nd + 6];
+            for (int c = 0; c < 6; ++c) o[6 + c] = q64[8 * nd + c];
+            o[12] = leaf ? 1.0 : 0.0;
+            o[13] = (leaf && cnt == 1) ? static_cast<double>(ids[link[nd].x]) : -1.0;
+            o[14] = 0.0;
+            o[15] = leaf ? cnt : -1.0;
+        }
+        ++count;
+        if (link[nd].y > 0)
+            for (int k = link[nd].y - 1; k >= 0; --k) stackv.push_back(link[nd].x + k);
+    }
+    if (n_rows) *n_rows = count;
+    return NEXT_OK;
+}
+
+int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                    uint32_t* vals_out, int key_bits) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (n < 0 || n >= (int64_t(1) << 30) || key_bits < 1 || key_bits > 64 || (n > 0 && (!keys_in || !vals_in)))
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad sort arguments");
+    if (n == 0) return NEXT_OK;
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "set device");
+    uint64_t *k0 = nullptr, *k1 = nullptr;
+    uint32_t *v0 = nullptr, *v1 = nullptr, *scr = nullptr;
+    auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
+    A(&k0, n); A(&k1, n); A(&v0, n); A(&v1, n); A(&scr, sort_scratch_words(n));
+    bool in_alt = false;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(k0, keys_in, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v0, vals_in, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, h->st);
+    if (e == cudaSuccess) e = radix_sort_pairs(k0, v0, k1, v1, n, key_bits, scr, h->err, &in_alt, h->st);
+    if (e == cudaSuccess && keys_out)
+        e = cudaMemcpyAsync(keys_out, in_alt ? k1 : k0, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess && vals_out)
+        e = cudaMemcpyAsync(vals_out, in_alt ? v1 : v0, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
+    int bits = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&bits, h->err, sizeof(int), cudaMemcpyDeviceToHost);
+    dfree(k0); dfree(k1); dfree(v0); dfree(v1); dfree(scr);
+    if (e != cudaSuccess) return cuda_fail(h, e, "sort");
+    if (bits & kErrSort) return fail(h, NEXT_ERR_DEVICE, "sort look-back timeout");
+    return NEXT_OK;
+}
+
+int next_fp32_peak(int device, double* tflops, double* sm_mhz_hint) {
+    if (!tflops) return NEXT_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return NEXT_ERR_CUDA;
+    int sms = 0, khz = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, device);
+    float* out = nullptr;
+    if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) return NEXT_ERR_OUT_OF_MEMORY;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = sms * 8, iters = 4096;
+    double best = 0.0;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a, 0);
+        launch_fma_peak(out, blocks, iters, 0);
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double flops = 2.0 * 8.0 * 16.0 * iters * 256.0 * blocks;
+        if (rep > 0 && ms > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    *tflops = best;
+    if (sm_mhz_hint) *sm_mhz_hint = khz / 1000.0;
+    return cudaGetLastError() == cudaSuccess ? NEXT_OK : NEXT_ERR_CUDA;
+}
+
+void* next_host_alloc(int64_t bytes) {
+    void* p = nullptr;
+    if (bytes <= 0 || cudaHostAlloc(&p, static_cast<size_t>(bytes), cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void next_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
+int64_t next_kernel_launches(void) { return launches_so_far(); }
+
+int next_flush_l2(next_handle* h) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (!h->flush) {
+        h->flush_bytes = size_t(256) << 20;
+        NB_TRY(cudaMalloc(&h->flush, h->flush_bytes), "flush buffer");
+    }
+    static unsigned char v = 0;
+    NB_TRY(cudaMemsetAsync(h->flush, ++v, h->flush_bytes, h->st), "flush");
+    return NEXT_OK;
+}
+
+}  // extern "C"

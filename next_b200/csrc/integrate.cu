@@ -1,0 +1,300 @@
+// KDK leapfrog updates, body reordering, the adaptive time step, FP64
+// diagnostics, and the host<->device staging kernels.
+//
+// Built with -fmad=false: v += a*(dt/2) and x += v*dt round the product and
+// the sum separately, as the reference's loops do (src/gravity/step.h:120-122,
+// 143-145), so reference-mode trajectories match it bit for bit.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nb {
+
+namespace {
+
+__global__ void gather_bodies_kernel(Bodies src, Bodies dst, const uint32_t* __restrict__ idx, int64_t n,
+                                     uint32_t* __restrict__ inv, int* err) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t j = idx[p];
+    if (j >= n) { raise_error(err, kErrIndex); return; }
+    dst.x[p] = src.x[j]; dst.y[p] = src.y[j]; dst.z[p] = src.z[j];
+    dst.vx[p] = src.vx[j]; dst.vy[p] = src.vy[j]; dst.vz[p] = src.vz[j];
+    dst.m[p] = src.m[j];
+    dst.type[p] = src.type[j];
+    const uint32_t id = src.id[j];
+    dst.id[p] = id;
+    inv[id] = static_cast<uint32_t>(p);
+}
+
+__global__ void kick_drift_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err) {
+    if (*err & kErrAbort) return;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double dt = dts[0], half = dts[1];
+    double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+    vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
+    b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
+    b.x[i] += vx * dt; b.y[i] += vy * dt; b.z[i] += vz * dt;
+}
+
+__global__ void kick_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err) {
+    if (*err & kErrAbort) return;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double half = dts[1];
+    b.vx[i] += b.ax[i] * half; b.vy[i] += b.ay[i] * half; b.vz[i] += b.az[i] * half;
+}
+
+// computeAdaptiveDt (src/dt/adaptive.h:23-52): the largest squared speed is
+// an exact max, so the order of the reduction does not change the result.
+__global__ void __launch_bounds__(256)
+adaptive_dt_kernel(const double* __restrict__ vx, const double* __restrict__ vy, const double* __restrict__ vz,
+                   int64_t n, double base_dt, double* partial, unsigned int* ticket, double* out) {
+    double mx = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double s2 = vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i];
+        if (s2 > mx) mx = s2;
+    }
+    __shared__ double sm[8];
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) b = fmax(b, sm[w]);
+        partial[blockIdx.x] = b;
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double v2 = 0.0;
+    for (unsigned k = 0; k < gridDim.x; ++k) v2 = fmax(v2, __ldcg(partial + k));
+    *ticket = 0u;
+    double v = sqrt(v2);
+    v = v < 1e4 ? v : 1e4;
+    double dt;
+    if (v < 1e-8) {
+        dt = base_dt;
+    } else {
+        dt = base_dt / (1 + v);
+        const double lo = base_dt * 0.01, hi = base_dt * 1.0;
+        dt = (dt < lo) ? lo : dt;
+        dt = (hi < dt) ? hi : dt;
+    }
+    out[0] = dt;
+    out[1] = dt * 0.5;
+}
+
+// Kinetic energy, potential energy, momentum, angular momentum (FP64).
+__global__ void __launch_bounds__(256)
+diagnostics_kernel(Bodies b, int64_t n, bool have_pot, double* partial, unsigned int* ticket, double* out) {
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double m = b.m[i], vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+        const double x = b.x[i], y = b.y[i], z = b.z[i];
+        s[0] += 0.5 * m * (vx * vx + vy * vy + vz * vz);
+        if (have_pot) s[1] += 0.5 * m * b.pot[i];
+        s[2] += m * vx; s[3] += m * vy; s[4] += m * vz;
+        s[5] += m * (y * vz - z * vy);
+        s[6] += m * (z * vx - x * vz);
+        s[7] += m * (x * vy - y * vx);
+    }
+    __shared__ double sm[8][8];
+    for (int c = 0; c < 8; ++c) {
+        double v = s[c];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) sm[c][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < 8; ++c) {
+            double v = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sm[c][w];
+            partial[8 * blockIdx.x + c] = v;
+        }
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    for (int c = 0; c < 8; ++c) {
+        double v = 0.0;
+        for (unsigned k = 0; k < gridDim.x; ++k) v += __ldcg(partial + 8 * k + c);
+        out[c] = v;
+    }
+    *ticket = 0u;
+}
+
+// Upload support: did positions, masses or types change?  Compared through
+// inv (caller index -> working position).
+__global__ void compare_kernel(const double* __restrict__ stage, const int* __restrict__ stype, Bodies b,
+                               const uint32_t* __restrict__ inv, int64_t n, int* changed) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = inv[i];
+    const bool same = stage[i] == b.x[p] && stage[n + i] == b.y[p] && stage[2 * n + i] == b.z[p] &&
+                      stage[6 * n + i] == b.m[p] && stype[i] == b.type[p];
+    if (!same) *changed = 1;
+}
+
+__global__ void load_velocities_kernel(const double* __restrict__ stage, Bodies b, const uint32_t* __restrict__ inv,
+                                       int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = inv[i];
+    b.vx[p] = stage[3 * n + i]; b.vy[p] = stage[4 * n + i]; b.vz[p] = stage[5 * n + i];
+}
+
+__global__ void load_all_kernel(const double* __restrict__ stage, const int* __restrict__ stype, Bodies b,
+                                uint32_t* __restrict__ inv, int64_t n) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    b.x[i] = stage[i]; b.y[i] = stage[n + i]; b.z[i] = stage[2 * n + i];
+    b.vx[i] = stage[3 * n + i]; b.vy[i] = stage[4 * n + i]; b.vz[i] = stage[5 * n + i];
+    b.m[i] = stage[6 * n + i];
+    b.type[i] = stype[i];
+    b.id[i] = static_cast<uint32_t>(i);
+    inv[i] = static_cast<uint32_t>(i);
+    b.ax[i] = 0.0; b.ay[i] = 0.0; b.az[i] = 0.0;
+}
+
+// Download support: gather `count` FP64 lanes into caller order.
+__global__ void gather_out_kernel(const double* const* __restrict__ lanes, int count,
+                                  const uint32_t* __restrict__ inv, int64_t n, double* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = inv[i];
+    for (int c = 0; c < count; ++c) out[c * n + i] = lanes[c][p];
+}
+
+__global__ void ids_to_positions_kernel(const int64_t* __restrict__ ids, const uint32_t* __restrict__ inv, int64_t k,
+                                        int64_t* __restrict__ pos) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < k) pos[t] = inv[ids[t]];
+}
+
+__global__ void set_dt_kernel(double* dts, double dt) {
+    dts[0] = dt;
+    dts[1] = dt * 0.5;
+}
+
+// FP32 FMA throughput probe: 8 independent chains per thread.
+__global__ void __launch_bounds__(256) fma_peak_kernel(float* out, int iters, float a, float b) {
+    float r[8];
+    for (int k = 0; k < 8; ++k) r[k] = threadIdx.x * 1e-3f + k;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int u = 0; u < 16; ++u)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) r[k] = fmaf(r[k], a, b);
+    }
+    float s = 0.f;
+    for (int k = 0; k < 8; ++k) s += r[k];
+    if (s == 1.2345f) out[0] = s;   // keeps the chains live
+}
+
+inline unsigned grid_for(int64_t n, int threads) { return static_cast<unsigned>((n + threads - 1) / threads); }
+
+}  // namespace
+
+cudaError_t launch_gather_bodies(const Bodies& src, const Bodies& dst, const uint32_t* idx, int64_t n, uint32_t* inv,
+                                 int* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    gather_bodies_kernel<<<grid_for(n, 256), 256, 0, st>>>(src, dst, idx, n, inv, err);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kick_drift(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    kick_drift_kernel<<<grid_for(n, 256), 256, 0, st>>>(b, n, dts, err);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    kick_kernel<<<grid_for(n, 256), 256, 0, st>>>(b, n, dts, err);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+int reduce_blocks(int64_t n) {
+    int64_t b = (n + 256 * 8 - 1) / (256 * 8);
+    if (b < 1) b = 1;
+    if (b > 1024) b = 1024;
+    return static_cast<int>(b);
+}
+
+cudaError_t launch_adaptive_dt(const Bodies& b, int64_t n, double base_dt, double* partial, unsigned int* ticket,
+                               double* out, cudaStream_t st) {
+    adaptive_dt_kernel<<<reduce_blocks(n), 256, 0, st>>>(b.vx, b.vy, b.vz, n, base_dt, partial, ticket, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_diagnostics(const Bodies& b, int64_t n, bool have_pot, double* partial, unsigned int* ticket,
+                               double* out, cudaStream_t st) {
+    diagnostics_kernel<<<reduce_blocks(n), 256, 0, st>>>(b, n, have_pot, partial, ticket, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compare(const double* stage, const int* stype, const Bodies& b, const uint32_t* inv, int64_t n,
+                           int* changed, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    compare_kernel<<<grid_for(n, 256), 256, 0, st>>>(stage, stype, b, inv, n, changed);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_load_velocities(const double* stage, const Bodies& b, const uint32_t* inv, int64_t n,
+                                   cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    load_velocities_kernel<<<grid_for(n, 256), 256, 0, st>>>(stage, b, inv, n);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_load_all(const double* stage, const int* stype, const Bodies& b, uint32_t* inv, int64_t n,
+                            cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    load_all_kernel<<<grid_for(n, 256), 256, 0, st>>>(stage, stype, b, inv, n);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_out(const double* const* lanes_dev, int count, const uint32_t* inv, int64_t n,
+                              double* out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    gather_out_kernel<<<grid_for(n, 256), 256, 0, st>>>(lanes_dev, count, inv, n, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ids_to_positions(const int64_t* ids, const uint32_t* inv, int64_t k, int64_t* pos,
+                                    cudaStream_t st) {
+    if (k <= 0) return cudaSuccess;
+    ids_to_positions_kernel<<<grid_for(k, 256), 256, 0, st>>>(ids, inv, k, pos);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_dt(double* dts, double dt, cudaStream_t st) {
+    set_dt_kernel<<<1, 1, 0, st>>>(dts, dt);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fma_peak(float* out, int blocks, int iters, cudaStream_t st) {
+    fma_peak_kernel<<<blocks, 256, 0, st>>>(out, iters, 0.9999999f, 1e-7f);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace nb

@@ -1,0 +1,215 @@
+// Stable LSD radix sort of (uint64 key, uint32 value) pairs: one histogram
+// pass over the keys for all digits, then one "onesweep" pass per 8-bit
+// digit.  Each onesweep pass ranks a tile of keys in shared memory (warp
+// match-any multisplit), publishes the tile's per-digit counts, and finds
+// the counts of all earlier tiles by decoupled look-back over a status
+// array (flag + count packed in one 32-bit word), so a pass reads and
+// writes every pair exactly once.  Tiles are numbered in the order blocks
+// start (an atomic ticket), so every tile a block waits on is already
+// running; each wait is still bounded and raises NEXT_DEVERR_SORT_TIMEOUT
+// instead of spinning forever.
+//
+// Memory bound: per pass 12 B read + 12 B written per pair.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nb {
+
+namespace {
+
+constexpr int kRadix = 256;
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 15;
+constexpr int kTile = kThreads * kItems;   // 3840 pairs
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kCountMask = (1u << 30) - 1;
+constexpr int kSpinLimit = 1 << 20;
+
+__global__ void __launch_bounds__(kThreads)
+histogram_kernel(const uint64_t* __restrict__ keys, int64_t n, int passes, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t local[8][kRadix];
+    for (int i = threadIdx.x; i < 8 * kRadix; i += kThreads) (&local[0][0])[i] = 0;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
+        const uint64_t k = keys[i];
+        for (int p = 0; p < passes; ++p) atomicAdd(&local[p][(k >> (8 * p)) & 0xff], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
+        const uint32_t v = (&local[0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Exclusive scan of each pass's 256 digit counts (one block per pass).
+__global__ void __launch_bounds__(kRadix) digit_offsets_kernel(const uint32_t* hist, uint32_t* offsets) {
+    __shared__ uint32_t s[kRadix];
+    const int p = blockIdx.x, t = threadIdx.x;
+    s[t] = hist[p * kRadix + t];
+    __syncthreads();
+    for (int o = 1; o < kRadix; o <<= 1) {
+        const uint32_t v = t >= o ? s[t - o] : 0u;
+        __syncthreads();
+        s[t] += v;
+        __syncthreads();
+    }
+    offsets[p * kRadix + t] = s[t] - hist[p * kRadix + t];
+}
+
+struct SortSmem {
+    uint32_t warp_hist[kWarps][kRadix];
+    uint32_t tile_start[kRadix];
+    uint32_t global_base[kRadix];
+    uint64_t keys[kTile];
+    uint32_t vals[kTile];
+    int tile;
+};
+
+__global__ void __launch_bounds__(kThreads)
+onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
+                const uint32_t* __restrict__ digit_offsets, uint32_t* status, unsigned int* tile_ticket,
+                int* err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.warp_hist[0][0])[i] = 0;
+    if (threadIdx.x == 0) S.tile = static_cast<int>(atomicAdd(tile_ticket, 1u));
+    __syncthreads();
+    const int tile = S.tile;
+    const int64_t tile_base = static_cast<int64_t>(tile) * kTile;
+    const int64_t warp_base = tile_base + static_cast<int64_t>(w) * kItems * 32;
+
+    uint64_t key[kItems];
+    uint32_t val[kItems];
+    int dig[kItems];
+    uint32_t rank[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const int64_t g = warp_base + k * 32 + lane;
+        if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; dig[k] = static_cast<int>((key[k] >> shift) & 0xff); }
+        else { key[k] = ~0ull; val[k] = 0u; dig[k] = kRadix - 1; }
+    }
+    // Warp-level multisplit in item order (stable: item k of every lane
+    // precedes item k+1, lanes in order within an item).
+    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint32_t peers = __match_any_sync(0xffffffffu, dig[k]);
+        const uint32_t before = S.warp_hist[w][dig[k]];
+        rank[k] = before + __popc(peers & lt);
+        __syncwarp();
+        if ((peers & lt) == 0) S.warp_hist[w][dig[k]] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // Per digit: exclusive prefix over warps, tile count, look-back.
+    const int d = threadIdx.x;
+    uint32_t count = 0;
+    for (int ww = 0; ww < kWarps; ++ww) {
+        const uint32_t c = S.warp_hist[ww][d];
+        S.warp_hist[ww][d] = count;
+        count += c;
+    }
+    volatile uint32_t* vstat = status;
+    if (tile == 0) vstat[d] = kFlagInc | count;
+    else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int pred = tile - 1;
+        while (pred >= 0) {
+            uint32_t v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+            int spins = 0;
+            while ((v & (kFlagAgg | kFlagInc)) == 0) {
+                if (++spins > kSpinLimit) { raise_error(err, kErrSort); break; }
+                v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+            }
+            excl += v & kCountMask;
+            if ((v & kFlagInc) || spins > kSpinLimit) break;
+            --pred;
+        }
+        vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
+    }
+    S.global_base[d] = digit_offsets[d] + excl;
+    // Exclusive scan of the tile counts over digits (local layout).
+    S.tile_start[d] = count;
+    __syncthreads();
+    for (int o = 1; o < kRadix; o <<= 1) {
+        const uint32_t v = d >= o ? S.tile_start[d - o] : 0u;
+        __syncthreads();
+        S.tile_start[d] += v;
+        __syncthreads();
+    }
+    S.tile_start[d] -= count;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const uint32_t pos = S.tile_start[dig[k]] + S.warp_hist[w][dig[k]] + rank[k];
+        S.keys[pos] = key[k];
+        S.vals[pos] = val[k];
+    }
+    __syncthreads();
+    const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
+    for (int i = threadIdx.x; i < valid; i += kThreads) {
+        const uint64_t k = S.keys[i];
+        const int dd = static_cast<int>((k >> shift) & 0xff);
+        const uint32_t gpos = S.global_base[dd] + (static_cast<uint32_t>(i) - S.tile_start[dd]);
+        if (gpos >= n) { raise_error(err, kErrIndex); continue; }
+        keys_out[gpos] = k;
+        vals_out[gpos] = S.vals[i];
+    }
+}
+
+}  // namespace
+
+size_t sort_scratch_words(int64_t n) {
+    const int64_t tiles = (n + kTile - 1) / kTile;
+    // hist + offsets (8 x 256 each), tile tickets (8), status (8 x tiles x 256)
+    return static_cast<size_t>(2 * 8 * kRadix + 8 + 8 * tiles * kRadix);
+}
+
+size_t sort_smem_bytes() { return sizeof(SortSmem); }
+
+cudaError_t sort_prepare() {
+    return cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(SortSmem)));
+}
+
+// Sorts (keys, vals) of length n using (alt_keys, alt_vals) as the other
+// half of the ping-pong.  The result lands in (keys, vals) when the number
+// of passes is even, else in (alt_keys, alt_vals); *in_alt tells which.
+// scratch holds sort_scratch_words(n) words.
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys, uint32_t* alt_vals,
+                             int64_t n, int key_bits, uint32_t* scratch, int* err, bool* in_alt,
+                             cudaStream_t st) {
+    *in_alt = false;
+    if (n <= 1) return cudaSuccess;
+    const int passes = (key_bits + 7) / 8;
+    const int64_t tiles = (n + kTile - 1) / kTile;
+    uint32_t* hist = scratch;
+    uint32_t* offsets = scratch + 8 * kRadix;
+    unsigned int* tickets = scratch + 16 * kRadix;
+    uint32_t* status = scratch + 16 * kRadix + 8;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * sort_scratch_words(n), st);
+    if (e != cudaSuccess) return e;
+    int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
+    if (hblocks > 1184) hblocks = 1184;
+    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys, n, passes, hist);
+    digit_offsets_kernel<<<passes, kRadix, 0, st>>>(hist, offsets);
+    uint64_t* src_k = keys; uint32_t* src_v = vals;
+    uint64_t* dst_k = alt_keys; uint32_t* dst_v = alt_vals;
+    for (int p = 0; p < passes; ++p) {
+        onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
+            src_k, src_v, dst_k, dst_v, n, 8 * p, offsets + p * kRadix,
+            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        uint64_t* tk = src_k; src_k = dst_k; dst_k = tk;
+        uint32_t* tv = src_v; src_v = dst_v; dst_v = tv;
+    }
+    *in_alt = (passes & 1) != 0;
+    count_launches(2 + passes);
+    return cudaGetLastError();
+}
+
+}  // namespace nb

@@ -1,0 +1,442 @@
+// Octree build from sorted octant keys, and the upward (moment) pass.
+//
+// A cell at level l is a run of sorted keys sharing their first l octant
+// digits.  With d[s] = shared-prefix level of keys s-1 and s (-1 where a
+// system starts), position s starts exactly the cells of levels > d[s]; the
+// cell (l, s) holds more than B bodies iff the next B keys all share l
+// digits with their predecessor, i.e. l <= min(d[s+1..s+B]).  So the
+// internal cells (more than B bodies, above the deepest level) starting at s
+// are the levels d[s]+1 .. min(min(d[s+1..s+B]), levels-1): counted per
+// position, scanned, and materialised in one pass each -- no level-by-level
+// loop.  For B = 1 this is exactly the tree the reference's one-body-per-
+// leaf insertion builds (src/gravity/octree.h:69-87).
+//
+// Numbering: internal cells get a depth-first id q (position, then level);
+// nodes are laid out sibling-contiguous (children of a node consecutive, in
+// octant order, system roots first) for the walks.
+//
+// Upward pass: one thread per leaf computes the leaf's moments, then climbs;
+// at each parent an atomic arrival counter elects the last child's thread to
+// combine all children in octant order (deterministic), and that thread
+// climbs on.  One launch, no per-level loop.
+//
+// Built with -fmad=false: every FP64 + and * rounds separately, so the
+// reference-mode moments repeat src/gravity/octree.h:92-127 bit for bit.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nb {
+
+namespace {
+
+__global__ void dlev_kernel(const uint64_t* __restrict__ keys, int64_t n, int base, int levels,
+                            int8_t* __restrict__ dlev) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    dlev[s] = static_cast<int8_t>(s == 0 ? -1 : shared_levels(keys[s - 1], keys[s], base, levels));
+}
+
+__global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf_cap, int levels,
+                            int32_t* __restrict__ nint) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    int mb = -1;
+    if (s + leaf_cap < n) {
+        mb = 127;
+        for (int j = 1; j <= leaf_cap; ++j) mb = min(mb, static_cast<int>(dlev[s + j]));
+    }
+    const int top = min(mb, levels - 1);
+    nint[s] = max(0, top - static_cast<int>(dlev[s]));
+}
+
+__device__ __forceinline__ int64_t lower_bound_key(const uint64_t* keys, int64_t lo, int64_t hi, uint64_t v) {
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int64_t upper_bound_key(const uint64_t* keys, int64_t lo, int64_t hi, uint64_t v) {
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (keys[mid] <= v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Walk groups from the children of one cell holding more than G bodies:
+// consecutive children of at most G bodies are packed while the total stays
+// <= G; a child of more than G bodies that is a leaf (deepest level) is cut
+// into chunks of G.  emit(start, count) is called per group; returns count.
+template <typename F>
+__device__ int pack_groups(const int32_t* b, int level, int levels, int leaf_cap, int group_cap, F emit) {
+    int ng = 0, run_start = -1, run_cnt = 0;
+    for (int c = 0; c < 8; ++c) {
+        const int cnt = b[c + 1] - b[c];
+        if (cnt == 0) continue;
+        if (cnt <= group_cap) {
+            if (run_start >= 0 && run_cnt + cnt <= group_cap) {
+                run_cnt += cnt;
+            } else {
+                if (run_start >= 0) { emit(run_start, run_cnt); ++ng; }
+                run_start = b[c]; run_cnt = cnt;
+            }
+        } else {
+            if (run_start >= 0) { emit(run_start, run_cnt); ++ng; run_start = -1; run_cnt = 0; }
+            const bool leaf = !(cnt > leaf_cap && level + 1 < levels);
+            if (leaf)
+                for (int o = 0; o < cnt; o += group_cap) { emit(b[c] + o, min(group_cap, cnt - o)); ++ng; }
+        }
+    }
+    if (run_start >= 0) { emit(run_start, run_cnt); ++ng; }
+    return ng;
+}
+
+__global__ void internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int8_t* __restrict__ dlev,
+                                const int32_t* __restrict__ int_base, const int32_t* __restrict__ sysid,
+                                const int64_t* __restrict__ offsets, int base, int levels, int leaf_cap,
+                                int group_cap, int64_t cap_int, Tree t, int* err) {
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int cnt = int_base[s + 1] - int_base[s];
+    if (cnt == 0) return;
+    const int d = dlev[s];
+    const int sys = sysid ? sysid[s] : 0;
+    int64_t e_prev = offsets ? offsets[sys + 1] : n;
+    const uint64_t ks = keys[s];
+    for (int k = 0; k < cnt; ++k) {
+        const int l = d + 1 + k;
+        const int64_t q = static_cast<int64_t>(int_base[s]) + k;
+        if (q >= t.cap_int) { raise_error(err, kErrTree); return; }
+        const int sh = base - 3 * l;                       // bits below level l's digits
+        const uint64_t low = (sh >= 64) ? ~0ull : ((1ull << sh) - 1ull);
+        const uint64_t prefix = ks & ~low;
+        const int64_t e = upper_bound_key(keys, s + 1, e_prev, prefix | low);
+        int32_t b[9];
+        b[0] = static_cast<int32_t>(s);
+        b[8] = static_cast<int32_t>(e);
+        const int csh = base - 3 * (l + 1);
+        int64_t lo = s;
+        for (int c = 1; c < 8; ++c) {
+            lo = lower_bound_key(keys, lo, e, prefix | (static_cast<uint64_t>(c) << csh));
+            b[c] = static_cast<int32_t>(lo);
+        }
+        int nchild = 0;
+        for (int c = 0; c < 8; ++c) nchild += b[c + 1] > b[c];
+        int ngroups = 0;
+        if (e - s > group_cap)
+            ngroups = pack_groups(b, l, levels, leaf_cap, group_cap, [](int, int) {});
+        t.int_start[q] = static_cast<int32_t>(s);
+        t.int_level[q] = static_cast<int8_t>(l);
+        for (int c = 0; c < 9; ++c) t.int_bounds[9 * q + c] = b[c];
+        t.int_packed[q] = static_cast<int64_t>(nchild) | (static_cast<int64_t>(ngroups) << 32);
+        e_prev = e;
+    }
+}
+
+__global__ void check_counts_kernel(int nsys, Tree t, int* err) {
+    const int64_t m = t.counts[0];
+    if (m > t.cap_int) { raise_error(err, kErrTree); t.counts[1] = nsys; t.counts[2] = nsys; return; }
+    const int64_t packed = t.int_packed[m];
+    const int64_t nodes = nsys + (packed & 0xffffffffll);
+    const int64_t groups = nsys + (packed >> 32);
+    if (nodes > t.cap_node || groups > t.cap_group) raise_error(err, kErrTree);
+    t.counts[1] = nodes < t.cap_node ? nodes : t.cap_node;
+    t.counts[2] = groups < t.cap_group ? groups : t.cap_group;
+}
+
+__global__ void roots_kernel(const int64_t* __restrict__ offsets, int64_t n, int nsys, int leaf_cap,
+                             int group_cap, Tree t) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nsys) return;
+    const int64_t b = offsets ? offsets[s] : 0;
+    const int64_t e = offsets ? offsets[s + 1] : n;
+    const int cnt = static_cast<int>(e - b);
+    if (cnt <= leaf_cap) {
+        t.link[s] = make_int2(static_cast<int>(b), -cnt);
+        t.parent[s] = -1;
+        t.level[s] = 0;
+    }
+    t.groups[s] = make_int4(static_cast<int>(b), cnt <= group_cap ? cnt : 0, s, 0);
+}
+
+__global__ void children_kernel(const uint64_t* __restrict__ keys, const int8_t* __restrict__ dlev,
+                                const int32_t* __restrict__ int_base, const int32_t* __restrict__ sysid,
+                                int nsys, int levels, int leaf_cap, int group_cap, Tree t, int* err) {
+    if (*err & kErrAbort) return;
+    const int64_t m = t.counts[0];
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+        const int l = t.int_level[q];
+        const int s = t.int_start[q];
+        int32_t b[9];
+        for (int c = 0; c < 9; ++c) b[c] = t.int_bounds[9 * q + c];
+        const int64_t pk = t.int_packed[q], nx = t.int_packed[q + 1];
+        const int fc = nsys + static_cast<int>(pk & 0xffffffffll);
+        const int nc = static_cast<int>((nx & 0xffffffffll) - (pk & 0xffffffffll));
+        const int fg = nsys + static_cast<int>(pk >> 32);
+        const int sys = sysid ? sysid[s] : 0;
+        if (l == 0) {
+            t.int_node[q] = sys;
+            t.link[sys] = make_int2(fc, nc);
+            t.parent[sys] = -1;
+            t.level[sys] = 0;
+        }
+        int k = 0;
+        for (int c = 0; c < 8; ++c) {
+            const int cs = b[c], cnt = b[c + 1] - b[c];
+            if (cnt == 0) continue;
+            const int nid = fc + k++;
+            t.parent[nid] = static_cast<int32_t>(q);
+            t.level[nid] = static_cast<int8_t>(l + 1);
+            if (nid >= t.cap_node) { raise_error(err, kErrIndex); return; }
+            if (cnt > leaf_cap && l + 1 < levels) {
+                const int64_t q2 = static_cast<int64_t>(int_base[cs]) + (l + 1 - dlev[cs] - 1);
+                if (q2 <= q || q2 >= m) { raise_error(err, kErrIndex); return; }
+                t.int_node[q2] = nid;
+                const int64_t p2 = t.int_packed[q2], n2 = t.int_packed[q2 + 1];
+                t.link[nid] = make_int2(nsys + static_cast<int>(p2 & 0xffffffffll),
+                                        static_cast<int>((n2 & 0xffffffffll) - (p2 & 0xffffffffll)));
+            } else {
+                t.link[nid] = make_int2(cs, -cnt);
+            }
+        }
+        if (b[8] - b[0] > group_cap) {
+            int g = fg;
+            int4* groups = t.groups;
+            const int64_t gcap = t.cap_group;
+            pack_groups(b, l, levels, leaf_cap, group_cap, [&](int gs, int gc) {
+                if (g < gcap) groups[g] = make_int4(gs, gc, sys, 0);
+                ++g;
+            });
+        }
+    }
+}
+
+// ---- moments ---------------------------------------------------------------
+
+__device__ __forceinline__ double4 ldcg4(const double4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldcg(q), b = __ldcg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+struct Mom {
+    double m, cx, cy, cz, q[6];
+};
+
+__device__ __forceinline__ void store_moments(Tree& t, int nid, const Mom& a, double half, double rcrit,
+                                              double G, bool accurate) {
+    t.com[nid] = make_double4(a.cx, a.cy, a.cz, a.m);
+    double* q64 = t.quad64 + 8 * static_cast<int64_t>(nid);
+    for (int c = 0; c < 6; ++c) q64[c] = a.q[c];
+    q64[6] = half;
+    q64[7] = rcrit;
+    if (accurate) {
+        const float r2 = a.m > 0.0 ? static_cast<float>(rcrit * rcrit) : -1.0f;
+        t.box[nid] = make_float4(static_cast<float>(a.cx), static_cast<float>(a.cy), static_cast<float>(a.cz), r2);
+        t.quad32[2 * static_cast<int64_t>(nid)] =
+            make_float4(static_cast<float>(G * a.q[0]), static_cast<float>(G * a.q[1]),
+                        static_cast<float>(G * a.q[2]), static_cast<float>(G * a.q[3]));
+        t.quad32[2 * static_cast<int64_t>(nid) + 1] =
+            make_float4(static_cast<float>(G * a.q[4]), static_cast<float>(G * a.q[5]), 0.0f, 0.0f);
+    }
+}
+
+// Reference rules (src/gravity/octree.h:104-126) over a list of (m, x, y, z)
+// children in octant order; `size` is the cell's half-width.
+template <typename Get>
+__device__ Mom combine_ref(int count, double size, Get get) {
+    Mom a{};
+    double m = 0, cx = 0, cy = 0, cz = 0;
+    for (int k = 0; k < count; ++k) {
+        const double4 c = get(k);
+        if (c.w == 0) continue;
+        m += c.w;
+        cx += c.x * c.w; cy += c.y * c.w; cz += c.z * c.w;
+    }
+    if (m > 0) { cx /= m; cy /= m; cz /= m; }
+    for (int k = 0; k < count; ++k) {
+        const double4 c = get(k);
+        if (c.w == 0) continue;
+        const double rx = c.x - cx, ry = c.y - cy, rz = c.z - cz;
+        const double r2 = rx * rx + ry * ry + rz * rz + (size * size * 0.01);
+        const double mc = c.w;
+        a.q[0] += mc * (3.0 * rx * rx - r2);
+        a.q[1] += mc * (3.0 * ry * ry - r2);
+        a.q[2] += mc * (3.0 * rz * rz - r2);
+        a.q[3] += mc * (3.0 * rx * ry);
+        a.q[4] += mc * (3.0 * rx * rz);
+        a.q[5] += mc * (3.0 * ry * rz);
+    }
+    a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
+    return a;
+}
+
+// Geometric centre of the level-l cell holding `key` (the reference's child
+// centre rule, src/gravity/octree.h:56-64).
+__device__ double3 cell_centre(uint64_t key, int level, double4 cube, int base) {
+    double cx = cube.x, cy = cube.y, cz = cube.z, h = cube.w;
+    for (int l = 1; l <= level; ++l) {
+        const int d = key_digit(key, l, base);
+        const double hs = h * 0.5;
+        cx = cx + ((d & 1) ? hs : -hs);
+        cy = cy + ((d & 2) ? hs : -hs);
+        cz = cz + ((d & 4) ? hs : -hs);
+        h = hs;
+    }
+    return make_double3(cx, cy, cz);
+}
+
+__device__ double rcrit_of(const Mom& a, uint64_t key, int level, double4 cube, int base, double half,
+                           double theta) {
+    const double3 g = cell_centre(key, level, cube, base);
+    double ox = a.cx - g.x, oy = a.cy - g.y, oz = a.cz - g.z;
+    if (!(a.m > 0)) { ox = oy = oz = 0.0; }
+    return 2.0 * half / theta + sqrt(ox * ox + oy * oy + oz * oz);
+}
+
+__global__ void upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
+                              const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P,
+                              Tree t, int* err) {
+    if (*err & kErrAbort) return;
+    const bool accurate = P.physics == NEXT_PHYSICS_ACCURATE;
+    const int64_t nodes = t.counts[1];
+    const int64_t ninternal = t.counts[0];
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int2 lk = t.link[n];
+        if (lk.y > 0) continue;                    // internal: filled by a climbing thread
+        const int first = lk.x, cnt = -lk.y;
+        if (first < 0 || static_cast<int64_t>(first) + cnt > nbodies) { raise_error(err, kErrIndex); continue; }
+        const int lvl = t.level[n];
+        // an empty leaf can only be the root of an empty system (node id = system)
+        const int sys = sysid ? (cnt > 0 ? sysid[first] : static_cast<int>(n)) : 0;
+        const double4 cube = cubes[sys];
+        const double half = ldexp(cube.w, -lvl);
+        Mom a{};
+        double rcrit = 0.0;
+        if (!accurate) {
+            if (cnt == 1) {
+                a.m = bd.m[first]; a.cx = bd.x[first]; a.cy = bd.y[first]; a.cz = bd.z[first];
+            } else if (cnt > 1) {
+                a = combine_ref(cnt, half, [&](int k) {
+                    return make_double4(bd.x[first + k], bd.y[first + k], bd.z[first + k], bd.m[first + k]);
+                });
+            }
+        } else {
+            double m = 0, cx = 0, cy = 0, cz = 0;
+            for (int j = first; j < first + cnt; ++j) {
+                const double mj = bd.m[j];
+                m += mj; cx += mj * bd.x[j]; cy += mj * bd.y[j]; cz += mj * bd.z[j];
+            }
+            const uint64_t key = cnt > 0 ? keys[first] : 0ull;
+            if (m > 0) { cx /= m; cy /= m; cz /= m; }
+            else { const double3 g = cell_centre(key, lvl, cube, base); cx = g.x; cy = g.y; cz = g.z; }
+            for (int j = first; j < first + cnt; ++j) {
+                const double rx = bd.x[j] - cx, ry = bd.y[j] - cy, rz = bd.z[j] - cz;
+                const double r2 = rx * rx + ry * ry + rz * rz;
+                const double mj = bd.m[j];
+                a.q[0] += mj * (3.0 * rx * rx - r2); a.q[1] += mj * (3.0 * ry * ry - r2);
+                a.q[2] += mj * (3.0 * rz * rz - r2); a.q[3] += mj * (3.0 * rx * ry);
+                a.q[4] += mj * (3.0 * rx * rz);      a.q[5] += mj * (3.0 * ry * rz);
+            }
+            a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
+            rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
+        }
+        store_moments(t, static_cast<int>(n), a, half, rcrit, P.G, accurate);
+        // climb
+        int q = t.parent[n];
+        while (q >= 0) {
+            if (q >= ninternal) { raise_error(err, kErrIndex); break; }
+            const int nid = t.int_node[q];
+            if (nid < 0 || nid >= nodes) { raise_error(err, kErrIndex); break; }
+            const int2 plk = t.link[nid];
+            if (plk.y < 1 || plk.y > 8 || plk.x < 0 || static_cast<int64_t>(plk.x) + plk.y > nodes) {
+                raise_error(err, kErrIndex);
+                break;
+            }
+            __threadfence();
+            const int old = atomicAdd(t.counter + q, 1);
+            if (old != plk.y - 1) break;
+            t.counter[q] = 0;                      // re-armed for the next build
+            __threadfence();
+            const int pl = t.int_level[q];
+            const int ps = t.int_start[q];
+            const double4 pcube = cubes[sysid ? sysid[ps] : 0];
+            const double phalf = ldexp(pcube.w, -pl);
+            Mom p{};
+            double prc = 0.0;
+            if (!accurate) {
+                p = combine_ref(plk.y, phalf, [&](int k) { return ldcg4(t.com + plk.x + k); });
+            } else {
+                double m = 0, cx = 0, cy = 0, cz = 0;
+                for (int k = 0; k < plk.y; ++k) {
+                    const double4 c = ldcg4(t.com + plk.x + k);
+                    m += c.w; cx += c.w * c.x; cy += c.w * c.y; cz += c.w * c.z;
+                }
+                const uint64_t key = keys[ps];
+                if (m > 0) { cx /= m; cy /= m; cz /= m; }
+                else { const double3 g = cell_centre(key, pl, pcube, base); cx = g.x; cy = g.y; cz = g.z; }
+                for (int k = 0; k < plk.y; ++k) {
+                    const double4 c = ldcg4(t.com + plk.x + k);
+                    const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
+                    const double rx = c.x - cx, ry = c.y - cy, rz = c.z - cz;
+                    const double r2 = rx * rx + ry * ry + rz * rz;
+                    const double mk = c.w;
+                    p.q[0] += __ldcg(cq + 0) + mk * (3.0 * rx * rx - r2);
+                    p.q[1] += __ldcg(cq + 1) + mk * (3.0 * ry * ry - r2);
+                    p.q[2] += __ldcg(cq + 2) + mk * (3.0 * rz * rz - r2);
+                    p.q[3] += __ldcg(cq + 3) + mk * (3.0 * rx * ry);
+                    p.q[4] += __ldcg(cq + 4) + mk * (3.0 * rx * rz);
+                    p.q[5] += __ldcg(cq + 5) + mk * (3.0 * ry * rz);
+                }
+                p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
+                prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
+            }
+            store_moments(t, nid, p, phalf, prc, P.G, accurate);
+            q = t.parent[nid];
+        }
+    }
+}
+
+}  // namespace
+
+cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const int32_t* sysid,
+                       const Systems& sys, const int64_t* d_offsets, const Params& P, Tree& t,
+                       void* scan_tmp, int* err, cudaStream_t st) {
+    const int threads = 256;
+    const unsigned blocks = static_cast<unsigned>((n + threads - 1) / threads);
+    const int leaf_cap = P.physics == NEXT_PHYSICS_REFERENCE ? 1 : P.leaf_cap;
+    const int group_cap = P.group_cap < leaf_cap ? leaf_cap : P.group_cap;
+    const int32_t* sid = sys.n > 1 ? sysid : nullptr;
+    const int64_t* offs = sys.n > 1 ? d_offsets : nullptr;
+    if (n > 0) {
+        dlev_kernel<<<blocks, threads, 0, st>>>(keys, n, sys.base, sys.levels, t.dlev);
+        nint_kernel<<<blocks, threads, 0, st>>>(t.dlev, n, leaf_cap, sys.levels, t.nint);
+    }
+    cudaError_t e = exclusive_scan<int32_t>(t.nint, t.nint, n, nullptr, static_cast<int32_t*>(scan_tmp),
+                                            t.counts + 0, st);
+    if (e != cudaSuccess) return e;
+    if (n > 0)
+        internal_kernel<<<blocks, threads, 0, st>>>(keys, n, t.dlev, t.nint, sid, offs, sys.base, sys.levels,
+                                                    leaf_cap, group_cap, t.cap_int, t, err);
+    e = exclusive_scan<int64_t>(t.int_packed, t.int_packed, t.cap_int, t.counts + 0,
+                                static_cast<int64_t*>(scan_tmp), nullptr, st);
+    if (e != cudaSuccess) return e;
+    check_counts_kernel<<<1, 1, 0, st>>>(sys.n, t, err);
+    e = cudaMemsetAsync(t.int_node, 0xff, sizeof(int32_t) * t.cap_int, st);
+    if (e != cudaSuccess) return e;
+    roots_kernel<<<(sys.n + 127) / 128, 128, 0, st>>>(offs, n, sys.n, leaf_cap, group_cap, t);
+    const unsigned cblocks = static_cast<unsigned>((t.cap_int + threads - 1) / threads);
+    children_kernel<<<cblocks < 4096u ? (cblocks ? cblocks : 1u) : 4096u, threads, 0, st>>>(
+        keys, t.dlev, t.nint, sid, sys.n, sys.levels, leaf_cap, group_cap, t, err);
+    const unsigned ublocks = static_cast<unsigned>((t.cap_node + threads - 1) / threads);
+    Params Pu = P;
+    upward_kernel<<<ublocks < 8192u ? ublocks : 8192u, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu,
+                                                                         t, err);
+    count_launches(n > 0 ? 8 : 5);
+    return cudaGetLastError();
+}
+
+}  // namespace nb

@@ -1,0 +1,304 @@
+"""GPU parity: the CUDA path against the oracle and the reference's own outputs.
+
+Tolerances
+  * octant keys, sort order, tree topology, reference-mode moments: bit-exact
+  * reference physics, plain FP64 forces and trajectories: |a_gpu - a_ref| <=
+    1e-12 * max|a_ref| (same FP64 operations; only CUDA's cbrt/pow may differ
+    from the host libm in the last bit)
+  * accurate physics, plain FP64 vs the oracle: 1e-12 relative
+  * mixed precision vs FP64 direct summation: median relative error <= 1e-3
+    (theta = 0.5, quadrupole), 99th percentile <= 1e-2
+"""
+import numpy as np
+import pytest
+
+from golden_cases import NAMES, load
+from next_b200 import ic
+from next_b200.native import Simulation
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_err(a, b):
+    num = np.sqrt(sum((a[c] - b[c]) ** 2 for c in ("ax", "ay", "az")))
+    den = np.sqrt(sum(b[c] ** 2 for c in ("ax", "ay", "az")))
+    return num / np.where(den > 0, den, 1.0)
+
+
+def max_abs(a, b, keys):
+    return max(float(np.max(np.abs(np.asarray(a[k]) - np.asarray(b[k])))) for k in keys)
+
+
+def scale(a):
+    return float(np.max(np.sqrt(a["ax"] ** 2 + a["ay"] ** 2 + a["az"] ** 2))) or 1.0
+
+
+@pytest.fixture(scope="module")
+def ref_sim():
+    s = Simulation("reference", "fp64")
+    yield s
+    s.close()
+
+
+# ---- keys and sort ----------------------------------------------------------
+
+@pytest.mark.parametrize("name", NAMES)
+def test_keys_bit_exact_golden(oracle, ref_sim, name):
+    b, _ = load(name)
+    ref_sim.upload(b)
+    keys, cube = ref_sim.debug_keys()
+    np.testing.assert_array_equal(cube, oracle.root_cube(b))
+    np.testing.assert_array_equal(keys, oracle.keys(b))
+
+
+@pytest.mark.parametrize("n", [100_003, 1_000_000])
+def test_keys_bit_exact_large(oracle, ref_sim, n):
+    b = ic.hernquist(n, seed=4) if n > 200_000 else ic.plummer(n, seed=11)
+    ref_sim.upload(b)
+    keys, _ = ref_sim.debug_keys()
+    np.testing.assert_array_equal(keys, oracle.keys(b))
+
+
+@pytest.mark.parametrize("n,bits", [(1, 64), (2, 64), (3839, 63), (3840, 63), (3841, 63), (100_000, 64),
+                                    (1_000_003, 63), (65_536, 8), (200_000, 20)])
+def test_sort_matches_stable_sort(ref_sim, n, bits):
+    rng = np.random.default_rng(n + bits)
+    keys = rng.integers(0, 2 ** min(bits, 63), n, dtype=np.uint64)
+    if bits == 64:
+        keys = keys | (rng.integers(0, 2, n, dtype=np.uint64) << np.uint64(63))
+    if n > 10:
+        keys[: n // 3] = keys[0]           # many duplicates: stability matters
+    vals = np.arange(n, dtype=np.uint32)
+    ko, vo = ref_sim.sort_pairs(keys, vals, bits)
+    order = np.argsort(keys, kind="stable")
+    np.testing.assert_array_equal(ko, keys[order])
+    np.testing.assert_array_equal(vo, vals[order])
+
+
+def test_body_order_is_stable_key_order(oracle, ref_sim):
+    b = ic.plummer(50_000, seed=3)
+    ref_sim.upload(b)
+    perm = ref_sim.debug_order()
+    np.testing.assert_array_equal(perm, oracle.sort(oracle.keys(b)))
+
+
+# ---- reference physics (plain FP64) against the reference -------------------
+
+@pytest.mark.parametrize("name", NAMES)
+def test_tree_matches_reference_golden(ref_sim, name):
+    b, z = load(name)
+    ref_sim.upload(b)
+    mine = ref_sim.debug_tree()
+    ref = z["tree"]
+    assert mine.shape[0] == ref.shape[0]
+    np.testing.assert_array_equal(mine[:, :14], ref[:, :14])
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_forces_golden(ref_sim, name):
+    b, z = load(name)
+    ref_sim.upload(b)
+    a = ref_sim.accel()
+    ref = {c: z[c] for c in ("ax", "ay", "az")}
+    assert max_abs(a, ref, ("ax", "ay", "az")) <= 1e-12 * scale(ref)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_step_golden(name):
+    b, z = load(name)
+    sim = Simulation("reference", "fp64")
+    sim.upload(b)
+    for _ in range(int(z["nsteps"])):
+        sim.step(float(z["step_dt"]))
+    s = sim.download()
+    out = {c: z["out_" + c] for c in ("x", "y", "z", "vx", "vy", "vz")}
+    tol = 1e-12 * max(1.0, max(float(np.max(np.abs(out[c]))) for c in out))
+    assert max_abs(s, out, out.keys()) <= tol
+    sim.close()
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_adaptive_dt_golden(ref_sim, name):
+    b, z = load(name)
+    ref_sim.upload(b)
+    assert ref_sim.adaptive_dt(float(z["base_dt"])) == float(z["adaptive_dt"])
+
+
+def test_reference_forces_plummer_64k(oracle, ref_sim):
+    b = ic.plummer(65_536, seed=0)
+    b["type"][::5] = 1
+    ref_sim.upload(b)
+    a = ref_sim.accel()
+    r = oracle.accel(b, mode="ref")
+    assert max_abs(a, r, ("ax", "ay", "az")) <= 1e-12 * scale(r)
+
+
+# ---- accurate physics --------------------------------------------------------
+
+@pytest.mark.parametrize("leaf_cap", [1, 8])
+def test_accurate_plain_matches_oracle(oracle, leaf_cap):
+    b = ic.plummer(16_384, seed=2)
+    sim = Simulation("accurate", "fp64", theta=0.5, eps=0.01, leaf_cap=leaf_cap)
+    sim.upload(b)
+    a = sim.accel(potential=True)
+    r = oracle.accel(b, mode="accurate", theta=0.5, eps=0.01, leaf_cap=leaf_cap, potential=True)
+    assert max_abs(a, r, ("ax", "ay", "az")) <= 1e-12 * scale(r)
+    assert float(np.max(np.abs(a["pot"] - r["pot"]))) <= 1e-12 * float(np.max(np.abs(r["pot"])))
+    st = sim.stats()
+    assert st["pp_interactions"] == r["pp"] and st["pc_interactions"] == r["pc"]
+    sim.close()
+
+
+def test_direct_sum_matches_oracle(oracle):
+    b = ic.plummer(20_000, seed=5)
+    sim = Simulation("accurate", "mixed", eps=0.01)
+    sim.upload(b)
+    idx = np.arange(0, 20_000, 37)
+    d = sim.direct_accel(idx)
+    r = oracle.direct(b, idx, eps=0.01)
+    assert max_abs(d, r, ("ax", "ay", "az")) <= 1e-12 * scale(r)
+    sim.close()
+
+
+@pytest.mark.parametrize("maker,n,theta,eps", [
+    (ic.plummer, 16_384, 0.5, 0.01),
+    (ic.uniform_sphere, 65_536, 0.5, 0.005),
+    (ic.hernquist, 65_536, 0.7, 0.002),
+])
+def test_mixed_precision_force_error(oracle, maker, n, theta, eps):
+    b = maker(n)
+    sim = Simulation("accurate", "mixed", theta=theta, eps=eps)
+    sim.upload(b)
+    a = sim.accel()
+    idx = np.random.default_rng(0).choice(n, 1024, replace=False)
+    d = oracle.direct(b, idx, eps=eps)
+    e = rel_err({c: a[c][idx] for c in a}, d)
+    assert np.median(e) <= 1e-3
+    assert np.percentile(e, 99) <= 1e-2
+    assert sim.stats()["device_error"] == 0
+    sim.close()
+
+
+def test_mixed_close_to_plain_accurate():
+    b = ic.plummer(32_768, seed=6)
+    plain = Simulation("accurate", "fp64", theta=0.5, eps=0.01, leaf_cap=16)
+    mixed = Simulation("accurate", "mixed", theta=0.5, eps=0.01, leaf_cap=16)
+    plain.upload(b)
+    mixed.upload(b)
+    e = rel_err(mixed.accel(), plain.accel())
+    # different opening tests (group box vs body) -> truncation-level differences only
+    assert np.median(e) <= 1e-3
+    plain.close()
+    mixed.close()
+
+
+# ---- integration ---------------------------------------------------------------
+
+def test_upload_download_round_trip():
+    b = ic.plummer(10_000, seed=9)
+    sim = Simulation("accurate", "mixed")
+    sim.upload(b)
+    s = sim.download()
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(s[c], b[c])
+    sim.accel()           # reorders the bodies on the device
+    s = sim.download()
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(s[c], b[c])
+    sim.close()
+
+
+def test_mixed_steps_conserve_energy_and_momentum():
+    b = ic.plummer(32_768, seed=7)
+    sim = Simulation("accurate", "mixed", theta=0.5, eps=0.01)
+    sim.upload(b)
+    d0 = sim.diagnostics()
+    e0 = d0["kinetic"] + d0["potential"]
+    sim.steps(1e-3, 50)
+    d1 = sim.diagnostics()
+    e1 = d1["kinetic"] + d1["potential"]
+    assert abs(e1 - e0) / abs(e0) < 1e-4
+    # Barnes-Hut forces are not pairwise symmetric: momentum drifts at the force-error level
+    assert np.max(np.abs(d1["momentum"] - d0["momentum"])) < 2e-4
+    assert sim.stats()["device_error"] == 0
+    sim.close()
+
+
+def test_graph_steps_equal_eager_steps():
+    b = ic.plummer(20_000, seed=8)
+    a = Simulation("accurate", "mixed")
+    g = Simulation("accurate", "mixed")
+    a.upload(b)
+    g.upload(b)
+    for _ in range(6):
+        a.step(1e-3)
+    g.steps(1e-3, 6)
+    sa, sg = a.download(), g.download()
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(sa[c], sg[c])
+    a.close()
+    g.close()
+
+
+def test_reuse_forces_matches_recompute():
+    b = ic.plummer(20_000, seed=10)
+    r = Simulation("accurate", "fp64", leaf_cap=4, reuse_forces=True)
+    f = Simulation("accurate", "fp64", leaf_cap=4, reuse_forces=False)
+    r.upload(b)
+    f.upload(b)
+    for _ in range(3):
+        r.step(1e-3)
+        f.step(1e-3)
+    sr, sf = r.download(), f.download()
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(sr[c], sf[c])
+    r.close()
+    f.close()
+
+
+def test_ensemble_equals_independent_systems():
+    bodies, offs = ic.ensemble(n_systems=8, seed=3, nmin=500, nmax=5000)
+    for precision, leaf in (("fp64", 1), ("mixed", 16)):
+        ens = Simulation("accurate", precision, leaf_cap=leaf)
+        ens.upload(bodies, offsets=offs)
+        a = ens.accel()
+        for s in range(8):
+            sl = slice(offs[s], offs[s + 1])
+            one = Simulation("accurate", precision, leaf_cap=leaf)
+            one.upload({k: v[sl] for k, v in bodies.items()})
+            b1 = one.accel()
+            for c in ("ax", "ay", "az"):
+                np.testing.assert_array_equal(a[c][sl], b1[c])
+            one.close()
+        ens.close()
+
+
+def test_invalid_input_rejected():
+    from next_b200.native import NextError
+    b = ic.plummer(100, seed=1)
+    b["x"][3] = np.nan
+    sim = Simulation("accurate", "mixed")
+    with pytest.raises(NextError):
+        sim.upload(b)
+    b = ic.plummer(100, seed=1)
+    b["m"][5] = -1.0
+    with pytest.raises(NextError):
+        sim.upload(b)
+    with pytest.raises(NextError):
+        sim.step(1e-3)       # nothing uploaded
+    sim.close()
+
+
+def test_coincident_bodies_do_not_break_the_build():
+    # the reference recurses forever on duplicates (octree.h:69-87); here they
+    # share a deepest-level leaf
+    b = ic.plummer(4096, seed=12)
+    for k in ("x", "y", "z"):
+        b[k][100:164] = b[k][99]
+    for physics, precision in (("reference", "fp64"), ("accurate", "fp64"), ("accurate", "mixed")):
+        sim = Simulation(physics, precision)
+        sim.upload(b)
+        a = sim.accel()
+        assert all(np.all(np.isfinite(a[c])) for c in a)
+        assert sim.stats()["device_error"] == 0
+        sim.close()
