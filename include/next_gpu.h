@@ -181,6 +181,27 @@ int next_debug_tree(next_handle* h, double* rows, int64_t cap, int64_t* n_rows);
 int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const uint32_t* vals_in,
                     uint64_t* keys_out, uint32_t* vals_out, int key_bits);
 
+/* Allocation-free variant of next_sort_pairs, for callers that own all device
+ * memory themselves (a fixed per-GPU budget, their own pool allocator) or
+ * cannot afford the device-wide synchronisation cudaMalloc/cudaFree may cause
+ * mid-step.  It has no counterpart in the reference, which sorts nothing.
+ *
+ * Sorts n (key, value) pairs from caller-owned DEVICE buffers d_keys_in /
+ * d_vals_in into caller-owned DEVICE buffers d_keys_out / d_vals_out (stable,
+ * low key_bits bits significant); the inputs are left untouched and must not
+ * alias the outputs.  It allocates nothing: all scratch comes from one
+ * static device array sized for NEXT_SORT_NOALLOC_MAX_PAIRS pairs (about
+ * 14.3 MiB, reserved on every GPU that loads it until the process exits);
+ * larger n is rejected with NEXT_ERR_INVALID_ARGUMENT.  The first call on a
+ * device looks up that array's address and sets the sort kernel's shared-
+ * memory limit, so make it before any stream capture.  Work is queued on
+ * `stream` (a cudaStream_t; NULL = default stream) of the current device and
+ * the call returns after that stream has finished it.  Every call reuses the
+ * same array, so calls whose GPU work overlaps race: serialise them. */
+#define NEXT_SORT_NOALLOC_MAX_PAIRS 1048576
+int next_sort_pairs_noalloc(const uint64_t* d_keys_in, const uint32_t* d_vals_in, uint64_t* d_keys_out,
+                            uint32_t* d_vals_out, int64_t n, int key_bits, void* stream);
+
 /* Sustained FP32 FMA throughput of the device (TFLOP/s), by a chain-of-FMA
  * kernel; the denominator of the walk's roofline. */
 int next_fp32_peak(int device, double* tflops, double* sm_mhz_hint);

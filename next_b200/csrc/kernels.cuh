@@ -16,11 +16,18 @@ cudaError_t launch_keys(const Bodies& b, const int32_t* sysid, int64_t n, const 
                         uint32_t* idx, cudaStream_t st);
 
 // sort.cu
+constexpr int64_t kSortTile = 256 * 15;   // pairs per onesweep tile (threads x items)
+constexpr int64_t sort_scratch_words_for(int64_t n) {
+    return 2 * 8 * 256 + 8 + 8 * ((n + kSortTile - 1) / kSortTile) * 256;
+}
 size_t sort_scratch_words(int64_t n);
 size_t sort_smem_bytes();
 cudaError_t sort_prepare();
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys, uint32_t* alt_vals, int64_t n,
                              int key_bits, uint32_t* scratch, int* err, bool* in_alt, cudaStream_t st);
+cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                                uint32_t* vals_out, uint64_t* alt_keys, uint32_t* alt_vals, int64_t n, int key_bits,
+                                uint32_t* scratch, int* err, cudaStream_t st);
 
 // scan.cu
 template <typename T>

@@ -213,3 +213,50 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
 }
 
 }  // namespace nb
+
+namespace nb {
+
+static_assert(kSortTile == kTile, "tile size shared with the scratch-size formula");
+
+// Sorts n pairs from (keys_in, vals_in) into (keys_out, vals_out), never
+// writing the inputs: the passes alternate between the outputs and
+// (alt_keys, alt_vals), starting on whichever side makes the last pass land
+// in the outputs.  scratch holds sort_scratch_words(n) words, err one word.
+cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                                uint32_t* vals_out, uint64_t* alt_keys, uint32_t* alt_vals, int64_t n, int key_bits,
+                                uint32_t* scratch, int* err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (n == 1) {
+        cudaError_t e = cudaMemcpyAsync(keys_out, keys_in, sizeof(uint64_t), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(vals_out, vals_in, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+        return e;
+    }
+    const int passes = (key_bits + 7) / 8;
+    const int64_t tiles = (n + kTile - 1) / kTile;
+    uint32_t* hist = scratch;
+    uint32_t* offsets = scratch + 8 * kRadix;
+    unsigned int* tickets = scratch + 16 * kRadix;
+    uint32_t* status = scratch + 16 * kRadix + 8;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * sort_scratch_words(n), st);
+    if (e != cudaSuccess) return e;
+    int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
+    if (hblocks > 1184) hblocks = 1184;
+    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys_in, n, passes, hist);
+    digit_offsets_kernel<<<passes, kRadix, 0, st>>>(hist, offsets);
+    const uint64_t* src_k = keys_in;
+    const uint32_t* src_v = vals_in;
+    for (int p = 0; p < passes; ++p) {
+        const bool to_out = ((passes - 1 - p) & 1) == 0;
+        uint64_t* dst_k = to_out ? keys_out : alt_keys;
+        uint32_t* dst_v = to_out ? vals_out : alt_vals;
+        onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
+            src_k, src_v, dst_k, dst_v, n, 8 * p, offsets + p * kRadix,
+            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        src_k = dst_k;
+        src_v = dst_v;
+    }
+    count_launches(2 + passes);
+    return cudaGetLastError();
+}
+
+}  // namespace nb

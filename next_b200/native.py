@@ -68,6 +68,8 @@ SIGNATURES = {
     "next_host_alloc": (C.c_void_p, [C.c_int64]),
     "next_host_free": (None, [C.c_void_p]),
     "next_kernel_launches": (C.c_int64, []),
+    "next_sort_pairs_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int,
+                                          C.c_void_p]),
 }
 
 _LIB = None
