@@ -36,6 +36,9 @@ METRIC = "particle-steps/s at <=1e-3 median force err: FP32-mixed vs FP64 GPU vs
 WORKLOAD = dict(name="cold_collapse_uniform_sphere", n=1_048_576, eps=0.005, theta=0.5, dt=5e-4, seed=1)
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOPS_PP, FLOPS_PC = 20, 56
+# DRAM bytes (read + write) of one walk launch on this workload, from an ncu
+# capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
+WALK_DRAM_BYTES = 58.12e6
 
 
 def env_rank():
@@ -187,7 +190,8 @@ def run_ours(args):
     W = WORKLOAD
     bodies = ic.uniform_sphere(W["n"], seed=W["seed"])
     n = W["n"]
-    sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local)
+    sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, leaf_cap=args.leaf_cap,
+                     group_cap=args.group_cap, walk_warps=args.walk_warps, walk_stack=args.walk_stack)
     sim.upload(bodies)
     # warm-up (establishes tree/stack capacities and the force cache)
     for _ in range(args.warmup):
@@ -310,11 +314,15 @@ def run_ours(args):
         "graph_value": n * args.steps / graph_s,
         "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
         "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / n,
+        "pp_fraction": st["pp_interactions"] / max(1, st["pp_interactions"] + st["pc_interactions"]),
+        "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - 1,
+                 "bodies_per_group": n / max(1, st["n_groups"] - 1), "max_walk_stack": st["max_stack"]},
         "stage_ms_per_step": {"build": st["ms_build"] / args.steps, "sort": st["ms_sort"] / args.steps,
                               "walk": st["ms_walk"] / args.steps, "other": st["ms_other"] / args.steps},
         "energy_drift": abs(e1 - e0) / abs(e0),
         "roofline": {"bound": "fp32", "kernel": "walk_mixed_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": WALK_DRAM_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this workload",
                      "peak_source": "measured live by next_fp32_peak (FFMA chains); MEASURED_PEAKS.json has no FP32 entry",
                      "flops_per_launch": flops_walk, "ms_per_launch": walk_ms,
                      "flops_rule": "20 per body-body + 56 per body-cell interaction"},
@@ -341,6 +349,10 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--leaf-cap", type=int, default=None, help="bodies per leaf of the mixed walk's tree")
+    ap.add_argument("--group-cap", type=int, default=None, help="bodies per walk group (<= 32)")
+    ap.add_argument("--walk-warps", type=int, default=None, help="warps per block of the mixed walk")
+    ap.add_argument("--walk-stack", type=int, default=None, help="per-warp traversal stack entries")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

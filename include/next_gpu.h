@@ -76,7 +76,7 @@ typedef struct next_params {
     int group_cap;      /* bodies per walk group, <= 32 (mixed precision) */
     int quadrupole;     /* 1: monopole + quadrupole; 0: monopole only (accurate mode) */
     int reuse_forces;   /* 1: the first half-kick reuses a(x_n) from the previous step */
-    int walk_warps;     /* warps per block of the mixed walk */
+    int walk_warps;     /* warps per block of the mixed walk (1..4) */
     int walk_stack;     /* per-warp traversal stack entries of the mixed walk */
     int device;         /* CUDA device ordinal */
 } next_params;

@@ -529,7 +529,7 @@ int next_create(const next_params* p, next_handle** out) {
         (p->precision != NEXT_PRECISION_FP64 && p->precision != NEXT_PRECISION_MIXED) ||
         (p->precision == NEXT_PRECISION_MIXED && p->physics != NEXT_PHYSICS_ACCURATE) || !(p->theta > 0.0) ||
         !(p->eps >= 0.0) || !std::isfinite(p->eps) || !std::isfinite(p->G) || p->leaf_cap < 1 || p->leaf_cap > 64 ||
-        p->group_cap < 1 || p->group_cap > 32 || p->walk_warps < 1 || p->walk_warps > 8 || p->walk_stack < 64 ||
+        p->group_cap < 1 || p->group_cap > 32 || p->walk_warps < 1 || p->walk_warps > 4 || p->walk_stack < 64 ||
         p->walk_stack > (1 << 14) ||
         (p->precision == NEXT_PRECISION_MIXED && p->leaf_cap > p->group_cap))
         return NEXT_ERR_INVALID_ARGUMENT;

@@ -28,6 +28,23 @@ namespace nb {
 
 namespace {
 
+// Compile-time knobs of the evaluation loop (unroll depth of a full batch and
+// the minimum resident blocks the register allocation must allow).
+#ifndef NB_WALK_UNROLL
+#define NB_WALK_UNROLL 8
+#endif
+#ifndef NB_WALK_GENERIC_UNROLL
+#define NB_WALK_GENERIC_UNROLL 1
+#endif
+#ifndef NB_WALK_FIXED
+#define NB_WALK_FIXED 1
+#endif
+#ifndef NB_WALK_MIN_BLOCKS
+#define NB_WALK_MIN_BLOCKS 6
+#endif
+
+constexpr int kWalkUnroll = NB_WALK_UNROLL;
+constexpr int kWalkGenericUnroll = NB_WALK_GENERIC_UNROLL;
 constexpr int kPcCap = 64;
 constexpr int kPpChunk = 16;
 constexpr int kPpCap = 32 + 32 * kPpChunk;
@@ -61,11 +78,103 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t;
 }
 
-// Stage up to 32 cells and evaluate them for this lane's target.
+// One body-cell interaction (monopole + traceless quadrupole) from a staged
+// entry e[0] = (dx, dy, dz, G m) relative to the group centre, e[1] = G (Qxx Qyy
+// Qzz Qxy), e[2] = G (Qxz Qyz - -).  56 algorithmic flops.
+template <bool QUAD, bool POT>
+__device__ __forceinline__ void pc_term(const float4* e, const Target& T, float eps2, float& sx, float& sy,
+                                        float& sz, float& sp) {
+    const float4 a = e[0];
+    const float dx = a.x - T.tx, dy = a.y - T.ty, dz = a.z - T.tz;
+    const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    const float mr3 = a.w * rinv * rinv2;
+    if (QUAD) {
+        const float4 b = e[1];
+        const float4 c = e[2];
+        const float qdx = fmaf(c.x, dz, fmaf(b.w, dy, b.x * dx));
+        const float qdy = fmaf(c.y, dz, fmaf(b.y, dy, b.w * dx));
+        const float qdz = fmaf(b.z, dz, fmaf(c.y, dy, c.x * dx));
+        const float q = fmaf(dz, qdz, fmaf(dy, qdy, dx * qdx));
+        const float rinv5 = rinv2 * rinv2 * rinv;
+        const float c7 = 2.5f * q * (rinv5 * rinv2);
+        const float cc = mr3 + c7;
+        sx = fmaf(cc, dx, fmaf(-rinv5, qdx, sx));
+        sy = fmaf(cc, dy, fmaf(-rinv5, qdy, sy));
+        sz = fmaf(cc, dz, fmaf(-rinv5, qdz, sz));
+        if (POT) sp = fmaf(-0.5f * q, rinv5, fmaf(-a.w, rinv, sp));
+    } else {
+        sx = fmaf(mr3, dx, sx);
+        sy = fmaf(mr3, dy, sy);
+        sz = fmaf(mr3, dz, sz);
+        if (POT) sp = fmaf(-a.w, rinv, sp);
+    }
+}
+
+// One body-body interaction from a staged entry (dx, dy, dz, G m).  20 flops.
+template <bool SOFT, bool POT>
+__device__ __forceinline__ void pp_term(const float4* e, const Target& T, float eps2, float& sx, float& sy,
+                                        float& sz, float& sp) {
+    const float4 a = e[0];
+    const float dx = a.x - T.tx, dy = a.y - T.ty, dz = a.z - T.tz;
+    const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+    float rinv = rsqrtf(r2);
+    if (!SOFT) rinv = r2 > 0.f ? rinv : 0.f;     // the target itself, unsoftened
+    const float mr = a.w * rinv;
+    const float mr3 = mr * rinv * rinv;
+    sx = fmaf(mr3, dx, sx);
+    sy = fmaf(mr3, dy, sy);
+    sz = fmaf(mr3, dz, sz);
+    if (POT) sp -= r2 > eps2 ? mr : 0.f;          // no self term
+}
+
+// Entries [k0, k0 + N) of a staged batch (stride STRIDE float4 per entry),
+// with a compile-time trip count so the loop unrolls into immediate offsets.
+template <int N, int STRIDE, bool PC, bool F1, bool POT>
+__device__ __forceinline__ void run_fixed(const float4* stage, int k0, const Target& T, float eps2, float& sx,
+                                          float& sy, float& sz, float& sp) {
+    const float4* e = stage + STRIDE * k0;
+#pragma unroll kWalkUnroll
+    for (int k = 0; k < N; ++k) {
+        if (PC) pc_term<F1, POT>(e + STRIDE * k, T, eps2, sx, sy, sz, sp);
+        else pp_term<F1, POT>(e + STRIDE * k, T, eps2, sx, sy, sz, sp);
+    }
+}
+
+// Evaluate a staged batch of `count` entries for this lane's target: the
+// lane's slice takes entries [slice*count/nslices, ...).  A full, unsplit
+// batch (the common case) runs a loop with a compile-time trip count; split
+// and partial batches a plain loop.  Both stay compact: instruction-cache
+// misses cost more here than loop overhead.
+template <int STRIDE, bool PC, bool F1, bool POT>
+__device__ __forceinline__ void eval_batch(const float4* stage, int count, float eps2, bool active, int slice,
+                                           int nslices, Target& T) {
+    if (!active) return;
+    float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
+    if (NB_WALK_FIXED && count == 32 && nslices == 1) {
+        run_fixed<32, STRIDE, PC, F1, POT>(stage, 0, T, eps2, sx, sy, sz, sp);
+    } else {
+        const int chunk = (count + nslices - 1) / nslices;
+        const int k0 = slice * chunk;
+        const int k1 = min(count, k0 + chunk);
+#pragma unroll kWalkGenericUnroll
+        for (int k = k0; k < k1; ++k) {
+            if (PC) pc_term<F1, POT>(stage + STRIDE * k, T, eps2, sx, sy, sz, sp);
+            else pp_term<F1, POT>(stage + STRIDE * k, T, eps2, sx, sy, sz, sp);
+        }
+    }
+    kahan_add(T.ax, T.cx, sx);
+    kahan_add(T.ay, T.cy, sy);
+    kahan_add(T.az, T.cz, sz);
+    if (POT) kahan_add(T.pot, T.cp, sp);
+}
+
+// Stage up to 32 cells (one per lane) and evaluate them.
 template <bool QUAD, bool POT>
 __device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count, const Tree& t, double gcx,
-                                        double gcy, double gcz, float G, float eps2, bool active, Target& T,
-                                        int lane) {
+                                        double gcy, double gcz, float G, float eps2, bool active, int slice,
+                                        int nslices, Target& T, int lane) {
     if (lane < count) {
         const int node = list[lane];
         const double4 c = t.com[node];
@@ -77,82 +186,27 @@ __device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count
         }
     }
     __syncwarp();
-    if (active) {
-        float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-#pragma unroll 8
-        for (int k = 0; k < count; ++k) {
-            const float4 a = L.stage[3 * k];
-            const float dx = a.x - T.tx, dy = a.y - T.ty, dz = a.z - T.tz;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-            const float rinv = rsqrtf(r2);
-            const float rinv2 = rinv * rinv;
-            const float mr3 = a.w * rinv * rinv2;
-            if (QUAD) {
-                const float4 b = L.stage[3 * k + 1];   // Qxx Qyy Qzz Qxy
-                const float4 e = L.stage[3 * k + 2];   // Qxz Qyz
-                const float qdx = fmaf(e.x, dz, fmaf(b.w, dy, b.x * dx));
-                const float qdy = fmaf(e.y, dz, fmaf(b.y, dy, b.w * dx));
-                const float qdz = fmaf(b.z, dz, fmaf(e.y, dy, e.x * dx));
-                const float q = fmaf(dz, qdz, fmaf(dy, qdy, dx * qdx));
-                const float rinv5 = rinv2 * rinv2 * rinv;
-                const float c7 = 2.5f * q * (rinv5 * rinv2);
-                const float cc = mr3 + c7;
-                sx = fmaf(cc, dx, fmaf(-rinv5, qdx, sx));
-                sy = fmaf(cc, dy, fmaf(-rinv5, qdy, sy));
-                sz = fmaf(cc, dz, fmaf(-rinv5, qdz, sz));
-                if (POT) sp = fmaf(-0.5f * q, rinv5, fmaf(-a.w, rinv, sp));
-            } else {
-                sx = fmaf(mr3, dx, sx);
-                sy = fmaf(mr3, dy, sy);
-                sz = fmaf(mr3, dz, sz);
-                if (POT) sp = fmaf(-a.w, rinv, sp);
-            }
-        }
-        kahan_add(T.ax, T.cx, sx);
-        kahan_add(T.ay, T.cy, sy);
-        kahan_add(T.az, T.cz, sz);
-        if (POT) kahan_add(T.pot, T.cp, sp);
-    }
+    eval_batch<3, true, QUAD, POT>(L.stage, count, eps2, active, slice, nslices, T);
     __syncwarp();
 }
 
-// Stage up to 32 bodies and evaluate them for this lane's target.
+// Stage up to 32 bodies (one per lane) and evaluate them.
 template <bool SOFT, bool POT>
 __device__ __forceinline__ void eval_pp(WarpLists& L, const int* list, int count, const Bodies& bd, double gcx,
-                                        double gcy, double gcz, float G, float eps2, bool active, Target& T,
-                                        int lane) {
+                                        double gcy, double gcz, float G, float eps2, bool active, int slice,
+                                        int nslices, Target& T, int lane) {
     if (lane < count) {
         const int j = list[lane];
         L.stage[lane] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
                                     static_cast<float>(bd.z[j] - gcz), static_cast<float>(G * bd.m[j]));
     }
     __syncwarp();
-    if (active) {
-        float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-#pragma unroll 8
-        for (int k = 0; k < count; ++k) {
-            const float4 a = L.stage[k];
-            const float dx = a.x - T.tx, dy = a.y - T.ty, dz = a.z - T.tz;
-            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-            float rinv = rsqrtf(r2);
-            if (!SOFT) rinv = r2 > 0.f ? rinv : 0.f;     // the target itself, unsoftened
-            const float mr = a.w * rinv;
-            const float mr3 = mr * rinv * rinv;
-            sx = fmaf(mr3, dx, sx);
-            sy = fmaf(mr3, dy, sy);
-            sz = fmaf(mr3, dz, sz);
-            if (POT) sp -= r2 > eps2 ? mr : 0.f;          // no self term
-        }
-        kahan_add(T.ax, T.cx, sx);
-        kahan_add(T.ay, T.cy, sy);
-        kahan_add(T.az, T.cz, sz);
-        if (POT) kahan_add(T.pot, T.cp, sp);
-    }
+    eval_batch<1, false, SOFT, POT>(L.stage, count, eps2, active, slice, nslices, T);
     __syncwarp();
 }
 
 template <bool QUAD, bool SOFT, bool POT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(128, NB_WALK_MIN_BLOCKS)
 walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int stack_cap, unsigned int* queue,
                   unsigned long long* stats, int* err) {
     if (*err & kErrAbort) return;
@@ -179,8 +233,15 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrIndex);
             continue;
         }
-        const bool active = lane < nt;
-        const int i = grp.x + (active ? lane : 0);
+        // Groups of at most 16 bodies are evaluated by 2, 4, ... warp slices,
+        // each taking a share of every list batch; slices are summed at the end.
+        int nslices = 1;
+        while (nt * nslices * 2 <= 32) nslices *= 2;
+        const int width = 32 / nslices;
+        const int slice = lane / width;
+        const int tl = lane % width;
+        const bool active = tl < nt;
+        const int i = grp.x + (active ? tl : 0);
         const double px = bd.x[i], py = bd.y[i], pz = bd.z[i];
         // group bounding box (FP64), centre and half extents
         double lox = px, hix = px, loy = py, hiy = py, loz = pz, hiz = pz;
@@ -243,7 +304,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
             if (pc_n >= 32) {
-                eval_pc<QUAD, POT>(L, L.pc, 32, t, gcx, gcy, gcz, G, eps2, active, T, lane);
+                eval_pc<QUAD, POT>(L, L.pc, 32, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
                 g_pc += 32;
                 pc_n -= 32;
                 const int v = lane < pc_n ? L.pc[32 + lane] : 0;
@@ -264,7 +325,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
                 __syncwarp();
                 int head = 0;
                 while (pp_n - head >= 32) {
-                    eval_pp<SOFT, POT>(L, L.pp + head, 32, bd, gcx, gcy, gcz, G, eps2, active, T, lane);
+                    eval_pp<SOFT, POT>(L, L.pp + head, 32, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
                     g_pp += 32;
                     head += 32;
                 }
@@ -281,13 +342,23 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrStack);
             continue;
         }
-        if (pc_n > 0) { eval_pc<QUAD, POT>(L, L.pc, pc_n, t, gcx, gcy, gcz, G, eps2, active, T, lane); g_pc += pc_n; }
-        if (pp_n > 0) { eval_pp<SOFT, POT>(L, L.pp, pp_n, bd, gcx, gcy, gcz, G, eps2, active, T, lane); g_pp += pp_n; }
-        if (active) {
-            bd.ax[i] = static_cast<double>(T.ax) - static_cast<double>(T.cx);
-            bd.ay[i] = static_cast<double>(T.ay) - static_cast<double>(T.cy);
-            bd.az[i] = static_cast<double>(T.az) - static_cast<double>(T.cz);
-            if (POT && bd.pot) bd.pot[i] = static_cast<double>(T.pot) - static_cast<double>(T.cp);
+        if (pc_n > 0) { eval_pc<QUAD, POT>(L, L.pc, pc_n, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
+        if (pp_n > 0) { eval_pp<SOFT, POT>(L, L.pp, pp_n, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
+        double fx = static_cast<double>(T.ax) - static_cast<double>(T.cx);
+        double fy = static_cast<double>(T.ay) - static_cast<double>(T.cy);
+        double fz = static_cast<double>(T.az) - static_cast<double>(T.cz);
+        double fp = POT ? static_cast<double>(T.pot) - static_cast<double>(T.cp) : 0.0;
+        for (int o = width; o < 32; o <<= 1) {
+            fx += __shfl_xor_sync(0xffffffffu, fx, o);
+            fy += __shfl_xor_sync(0xffffffffu, fy, o);
+            fz += __shfl_xor_sync(0xffffffffu, fz, o);
+            if (POT) fp += __shfl_xor_sync(0xffffffffu, fp, o);
+        }
+        if (active && slice == 0) {
+            bd.ax[i] = fx;
+            bd.ay[i] = fy;
+            bd.az[i] = fz;
+            if (POT && bd.pot) bd.pot[i] = fp;
         }
         npp += g_pp * static_cast<unsigned long long>(nt);
         npc += g_pc * static_cast<unsigned long long>(nt);

@@ -12,7 +12,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libnext_b200.so")
+LIB_PATH = os.environ.get("NEXT_B200_LIB") or os.path.join(HERE, "lib", "libnext_b200.so")
 
 PHYSICS = {"reference": 0, "accurate": 1}
 PRECISION = {"fp64": 0, "mixed": 1}
