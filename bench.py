@@ -33,7 +33,6 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle-steps/s at <=1e-3 median force err: FP32-mixed vs FP64 GPU vs CPU"
-WORKLOAD = dict(name="cold_collapse_uniform_sphere", n=1_048_576, eps=0.005, theta=0.5, dt=5e-4, seed=1)
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
@@ -140,6 +139,7 @@ def time_cpu_reference(bodies, dt, budget_s, threads=None):
 
 
 def run_reference_arm(args):
+    WORKLOAD = CONFIGS["c2"]
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
@@ -174,9 +174,97 @@ def run_reference_arm(args):
     return 0
 
 
+CONFIGS = {
+    "c1": dict(name="plummer_16k", maker="plummer", n=16_384, seed=0, eps=0.01, theta=0.5, dt=1e-3),
+    "c2": dict(name="cold_collapse_uniform_sphere", maker="uniform_sphere", n=1_048_576, seed=1, eps=0.005,
+               theta=0.5, dt=5e-4),
+    "c3": dict(name="two_galaxy_encounter", maker="two_galaxies", n=4_194_304, seed=2, eps=0.01, theta=0.6, dt=1e-3),
+    "c4": dict(name="batched_plummer_ensemble_256", maker="ensemble", n=None, seed=3, eps=0.01, theta=0.5, dt=1e-3),
+    "c5": dict(name="hernquist_halo_16M", maker="hernquist", n=16_777_216, seed=4, eps=0.002, theta=0.7, dt=2.5e-4),
+}
+
+
+def make_bodies(cfg):
+    from next_b200 import ic
+    m = cfg["maker"]
+    if m == "uniform_sphere":
+        return ic.uniform_sphere(cfg["n"], seed=cfg["seed"]), None
+    if m == "plummer":
+        return ic.plummer(cfg["n"], seed=cfg["seed"]), None
+    if m == "hernquist":
+        return ic.hernquist(cfg["n"], seed=cfg["seed"]), None
+    if m == "two_galaxies":
+        return ic.two_galaxies(cfg["n"] // 2, seed=cfg["seed"]), None
+    return ic.ensemble(256, seed=cfg["seed"])
+
+
+def ensemble_error(bodies, offsets, a, cfg, device, k_systems=8):
+    """Force error of the batched walk on a sample of systems, each against its own FP64 direct sum."""
+    from next_b200.native import Simulation
+    rng = np.random.default_rng(777)
+    pick = rng.choice(len(offsets) - 1, k_systems, replace=False)
+    errs = []
+    for s in pick:
+        sl = slice(offsets[s], offsets[s + 1])
+        one = Simulation("accurate", "fp64", theta=cfg["theta"], eps=cfg["eps"], device=device)
+        one.upload({k: v[sl] for k, v in bodies.items()})
+        idx = np.arange(offsets[s + 1] - offsets[s])
+        d = one.direct_accel(idx)
+        num = np.sqrt(sum((a[c][sl] - d[c]) ** 2 for c in ("ax", "ay", "az")))
+        den = np.sqrt(sum(d[c] ** 2 for c in ("ax", "ay", "az")))
+        errs.append(num / den)
+        one.close()
+    e = np.concatenate(errs)
+    return {"median": float(np.median(e)), "p90": float(np.percentile(e, 90)), "p99": float(np.percentile(e, 99)),
+            "systems": int(k_systems)}
+
+
+def plain_fp64_leg(bodies, offsets, cfg, device, steps, idx):
+    """The plain FP64 GPU step (one thread per body, two tree builds per step)."""
+    from next_b200.native import Simulation
+    if offsets is None:
+        p = Simulation("accurate", "fp64", theta=cfg["theta"], eps=cfg["eps"], leaf_cap=1, reuse_forces=False,
+                       device=device)
+        p.upload(bodies)
+        p.step(cfg["dt"])
+        p.sync()
+        a_plain = p.accel()
+        err = force_error(a_plain, p.direct_accel(idx), idx)
+        p.reset_timers()
+        p.set_timing(True)
+        for _ in range(steps):
+            p.flush_l2()
+            p.step(cfg["dt"])
+        p.sync()
+        st = p.stats()
+        p.close()
+        n = bodies["x"].shape[0]
+        return {"value": n * steps / (st["ms_step"] * 1e-3), "steps": steps, "ms_per_step": st["ms_step"] / steps,
+                "force_error": err, "structure": "one thread per body, leaf_cap 1, two tree builds per step"}
+    # ensemble: loop the single-system plain FP64 step over a sample of systems
+    rng = np.random.default_rng(99)
+    pick = rng.choice(len(offsets) - 1, 16, replace=False)
+    bodies_done, ms = 0, 0.0
+    for s in pick:
+        sl = slice(offsets[s], offsets[s + 1])
+        p = Simulation("accurate", "fp64", theta=cfg["theta"], eps=cfg["eps"], leaf_cap=1, reuse_forces=False,
+                       device=device)
+        p.upload({k: v[sl] for k, v in bodies.items()})
+        p.step(cfg["dt"])
+        p.reset_timers()
+        p.set_timing(True)
+        for _ in range(steps):
+            p.step(cfg["dt"])
+        p.sync()
+        ms += p.stats()["ms_step"]
+        bodies_done += (offsets[s + 1] - offsets[s]) * steps
+        p.close()
+    return {"value": bodies_done / (ms * 1e-3), "steps": steps, "ms_per_step": None, "force_error": None,
+            "structure": "single-system plain FP64 step looped over 16 sampled systems (device time summed)"}
+
+
 def run_ours(args):
     rank, world, local = env_rank()
-    from next_b200 import ic
     from next_b200.native import Simulation, fp32_peak, load
     lib = load()
     dist = None
@@ -187,21 +275,27 @@ def run_ours(args):
         tdist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                  timeout=__import__("datetime").timedelta(seconds=120))
         dist = tdist
-    W = WORKLOAD
-    bodies = ic.uniform_sphere(W["n"], seed=W["seed"])
-    n = W["n"]
+    W = CONFIGS[args.config]
+    bodies, offsets = make_bodies(W)
+    n = bodies["x"].shape[0]
     sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, leaf_cap=args.leaf_cap,
                      group_cap=args.group_cap, walk_warps=args.walk_warps, walk_stack=args.walk_stack)
-    sim.upload(bodies)
-    # warm-up (establishes tree/stack capacities and the force cache)
+    sim.upload(bodies, offsets=offsets)
+    sim.step(W["dt"])
+    tune = None if args.no_autotune else sim.autotune()
+    # warm-up (capacities, force cache, clocks)
     for _ in range(args.warmup):
         sim.step(W["dt"])
     sim.sync()
     # force error vs FP64 direct summation at the current positions
-    idx = np.random.default_rng(12345).choice(n, 4096, replace=False)
+    idx = np.random.default_rng(12345).choice(n, min(4096, n), replace=False)
     a_mixed = sim.accel()
-    d = sim.direct_accel(idx)
-    err_mixed = force_error(a_mixed, d, idx)
+    if offsets is None:
+        err_mixed = force_error(a_mixed, sim.direct_accel(idx), idx)
+    else:
+        now = dict(bodies)
+        now.update(sim.download())          # the direct sums must see the current positions
+        err_mixed = ensemble_error(now, offsets, a_mixed, W, local)
     diag0 = sim.diagnostics()
     # ---- timed region: K steps, L2 flushed between steps, CUDA events per stage
     sim.reset_timers()
@@ -237,43 +331,23 @@ def run_ours(args):
     flops_walk = (FLOPS_PP * st["pp_interactions"] + FLOPS_PC * st["pc_interactions"]) / max(1, st["walk_launches"])
     peak = fp32_peak(local)
     achieved = flops_walk / (walk_ms * 1e-3) / 1e12
-    # ---- graph replay throughput of the same step (no per-stage events)
+    # ---- graph replay throughput of the same step (one captured graph per step)
     sim.sync()
-    import ctypes
     t0 = time.perf_counter()
     sim.steps(W["dt"], args.steps)
     sim.sync()
     graph_s = time.perf_counter() - t0
-    # ---- plain FP64 GPU step (reference step structure, accurate physics)
     fp64 = None
     if rank == 0 and not args.skip_fp64:
-        p = Simulation("accurate", "fp64", theta=W["theta"], eps=W["eps"], leaf_cap=1, reuse_forces=False, device=local)
-        p.upload(bodies)
-        p.step(W["dt"])
-        p.sync()
-        a_plain = p.accel()
-        dp = p.direct_accel(idx)
-        err_plain = force_error(a_plain, dp, idx)
-        p.reset_timers()
-        p.set_timing(True)
-        k64 = max(1, args.fp64_steps)
-        for _ in range(k64):
-            p.flush_l2()
-            p.step(W["dt"])
-        p.sync()
-        s64 = p.stats()
-        p.set_timing(False)
-        fp64 = {"value": n * k64 / (s64["ms_step"] * 1e-3), "steps": k64, "ms_per_step": s64["ms_step"] / k64,
-                "force_error": err_plain, "structure": "one thread per body, leaf_cap 1, two tree builds per step"}
-        p.close()
+        fp64 = plain_fp64_leg(bodies, offsets, W, local, max(1, args.fp64_steps), idx)
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
-    if rank == 0 and not args.skip_e2e:
+    if rank == 0 and not args.skip_e2e and offsets is None:
         import ctypes as C
-        bytes_lane = 8 * n
-        ptrs = [lib.next_host_alloc(bytes_lane) for _ in range(7)]
+        ptrs = [lib.next_host_alloc(8 * n) for _ in range(7)]
         lanes = [np.ctypeslib.as_array(C.cast(p_, C.POINTER(C.c_double)), shape=(n,)) for p_ in ptrs]
-        sim.download({k: lanes[i] for i, k in enumerate(("x", "y", "z", "vx", "vy", "vz"))})
+        names = ("x", "y", "z", "vx", "vy", "vz")
+        sim.download({k: lanes[i] for i, k in enumerate(names)})
         lanes[6][:] = bodies["m"]
         e_steps = max(3, args.steps // 4)
         sim.sync()
@@ -281,9 +355,9 @@ def run_ours(args):
         for _ in range(e_steps):
             sim.upload_arrays(lanes)
             sim.step(W["dt"])
-            sim.download({k: lanes[i] for i, k in enumerate(("x", "y", "z", "vx", "vy", "vz"))})
+            sim.download({k: lanes[i] for i, k in enumerate(names)})
         te = time.perf_counter() - t0
-        e2e = {"value": n * e_steps / te, "unit": "particle-steps/s", "h2d_bytes_per_step": 7 * 8 * n + 4 * 0,
+        e2e = {"value": n * e_steps / te, "unit": "particle-steps/s", "h2d_bytes_per_step": 7 * 8 * n,
                "d2h_bytes_per_step": 6 * 8 * n, "steps": e_steps,
                "path": "next_upload (pinned) + next_step + next_download (pinned) per step, host wall clock"}
         for p_ in ptrs:
@@ -291,7 +365,11 @@ def run_ours(args):
     # ---- CPU baseline: the reference's own Step() on the host cores
     cpu = None
     if rank == 0 and not args.skip_cpu:
-        cpu = time_cpu_reference(bodies, W["dt"], args.cpu_budget)
+        if offsets is None and n <= 2_000_000:
+            cpu = time_cpu_reference(bodies, W["dt"], args.cpu_budget)
+        else:
+            cpu = {"skipped": "one reference Step() at this size takes minutes on the host; see the c2 line"}
+    prm = sim.get_params()
     sim.close()
     if rank != 0:
         if dist:
@@ -302,26 +380,31 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 interactions / f64 state", "data": "synthetic",
-        "config": {"workload": W["name"], "n_bodies": n, "theta": W["theta"], "eps": W["eps"], "dt": W["dt"],
-                   "seed": W["seed"], "physics": "accurate (Plummer eps, full-width theta, corrected quadrupole)",
-                   "precision": "FP32-mixed", "leaf_cap": sim.params.leaf_cap, "group_cap": sim.params.group_cap,
+        "config": {"workload": W["name"], "n_bodies": n, "n_systems": 1 if offsets is None else len(offsets) - 1,
+                   "theta": W["theta"], "eps": W["eps"], "dt": W["dt"], "seed": W["seed"],
+                   "physics": "accurate (Plummer eps, full-width theta, corrected quadrupole)",
+                   "precision": "FP32-mixed", "leaf_cap": prm.leaf_cap, "group_cap": prm.group_cap,
+                   "walk_warps": prm.walk_warps, "walk_stack": prm.walk_stack,
+                   "autotuned": tune is not None,
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                    "l2": "flushed between steps (256 MiB write outside the timed events); step working set > L2"},
         "force_error": {"mixed": err_mixed, "fp64_plain": fp64["force_error"] if fp64 else None,
-                        "versus": "FP64 direct summation, 4096 seeded bodies"},
+                        "versus": "FP64 direct summation on seeded bodies"},
         "fp64_gpu": fp64,
         "speedup_vs_fp64_gpu": (value / world) / fp64["value"] if fp64 else None,
         "graph_value": n * args.steps / graph_s,
         "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
         "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / n,
         "pp_fraction": st["pp_interactions"] / max(1, st["pp_interactions"] + st["pc_interactions"]),
-        "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - 1,
-                 "bodies_per_group": n / max(1, st["n_groups"] - 1), "max_walk_stack": st["max_stack"]},
+        "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - st["n_systems"],
+                 "bodies_per_group": n / max(1, st["n_groups"] - st["n_systems"]), "max_walk_stack": st["max_stack"]},
         "stage_ms_per_step": {"build": st["ms_build"] / args.steps, "sort": st["ms_sort"] / args.steps,
                               "walk": st["ms_walk"] / args.steps, "other": st["ms_other"] / args.steps},
         "energy_drift": abs(e1 - e0) / abs(e0),
+        "autotune": tune,
         "roofline": {"bound": "fp32", "kernel": "walk_mixed_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": WALK_DRAM_BYTES,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "traffic": WALK_DRAM_BYTES if args.config == "c2" else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this workload",
                      "peak_source": "measured live by next_fp32_peak (FFMA chains); MEASURED_PEAKS.json has no FP32 entry",
                      "flops_per_launch": flops_walk, "ms_per_launch": walk_ms,
@@ -349,6 +432,8 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS), help="workload (default c2, the metric's)")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--leaf-cap", type=int, default=None, help="bodies per leaf of the mixed walk's tree")
     ap.add_argument("--group-cap", type=int, default=None, help="bodies per walk group (<= 32)")
     ap.add_argument("--walk-warps", type=int, default=None, help="warps per block of the mixed walk")

@@ -210,6 +210,21 @@ int next_fp32_peak(int device, double* tflops, double* sm_mhz_hint);
  * benchmarks that flush L2 between steps). */
 int next_flush_l2(next_handle* h);
 
+/* Autotuner (mixed precision): times the force phase (tree build + walk) on
+ * the uploaded bodies for leaf_cap x group_cap x walk_warps candidates, sizes
+ * walk_stack at 1.5x the deepest stack seen, and keeps the fastest setting in
+ * the handle.  Positions and velocities are not changed.  No counterpart in
+ * the reference (its tree has one body per leaf and no walk groups). */
+typedef struct next_tune_result {
+    int leaf_cap, group_cap, walk_warps, walk_stack;
+    double ms_force_phase;   /* device time of the chosen setting's force phase */
+    int candidates;          /* settings timed */
+} next_tune_result;
+int next_autotune(next_handle* h, next_tune_result* out);
+
+/* The handle's current parameters (after autotuning or capacity growth). */
+int next_get_params(const next_handle* h, next_params* p);
+
 /* Page-locked host memory for body arrays, so uploads and downloads run at
  * full PCIe/C2C bandwidth.  Free with next_host_free. */
 void* next_host_alloc(int64_t bytes);

@@ -1032,6 +1032,94 @@ void next_host_free(void* p) {
 
 int64_t next_kernel_launches(void) { return launches_so_far(); }
 
+int next_autotune(next_handle* h, next_tune_result* out) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (h->prm.precision != NEXT_PRECISION_MIXED)
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "autotuning applies to the mixed-precision walk");
+    struct Cand { int leaf, group, warps; };
+    std::vector<Cand> cands;
+    for (int g : {16, 24, 32})
+        for (int l : {8, 12, 16, 24})
+            for (int w : {2, 4})
+                if (l <= g) cands.push_back({l, g, w});
+    const Params saved_P = h->P;
+    const next_params saved_prm = h->prm;
+    cudaEvent_t a, b;
+    NB_TRY(cudaEventCreate(&a), "event");
+    NB_TRY(cudaEventCreate(&b), "event");
+    double best_ms = 1e300;
+    Cand best = {saved_P.leaf_cap, saved_P.group_cap, saved_prm.walk_warps};
+    int64_t best_stack = 0;
+    int tried = 0;
+    for (const Cand& c : cands) {
+        h->P.leaf_cap = c.leaf;
+        h->P.group_cap = c.group;
+        h->prm.leaf_cap = c.leaf;
+        h->prm.group_cap = c.group;
+        h->prm.walk_warps = c.warps;
+        drop_graphs(h);
+        // first pass sizes the tree and the stack (with recovery), second is timed
+        NB_TRY(cudaMemsetAsync(h->stats, 0, sizeof(unsigned long long) * 4, h->st), "stats");
+        rc = forces_checked(h, false);
+        if (rc) break;
+        NB_TRY(cudaEventRecord(a, h->st), "event");
+        rc = forces(h, false, nullptr);
+        if (rc) break;
+        NB_TRY(cudaEventRecord(b, h->st), "event");
+        int bits = 0;
+        rc = read_device_error(h, &bits);
+        if (rc) break;
+        if (bits) {
+            rc = recover(h, bits);
+            if (rc) break;
+            continue;
+        }
+        float ms = 0.f;
+        NB_TRY(cudaEventElapsedTime(&ms, a, b), "event time");
+        ++tried;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+            best_stack = static_cast<int64_t>(h->h_stats[2]);
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) {
+        h->P = saved_P;
+        h->prm = saved_prm;
+        return rc;
+    }
+    h->P.leaf_cap = best.leaf;
+    h->P.group_cap = best.group;
+    h->prm.leaf_cap = best.leaf;
+    h->prm.group_cap = best.group;
+    h->prm.walk_warps = best.warps;
+    // stack: 1.5x the deepest seen, in multiples of 64, at least 256
+    int64_t st = ((best_stack * 3 / 2 + 63) / 64) * 64;
+    h->prm.walk_stack = static_cast<int>(std::min<int64_t>(std::max<int64_t>(st, 256), 1 << 14));
+    drop_graphs(h);
+    rc = forces_checked(h, false);
+    if (rc) return rc;
+    NB_TRY(cudaMemsetAsync(h->stats, 0, sizeof(unsigned long long) * 4, h->st), "stats");
+    if (out) {
+        out->leaf_cap = best.leaf;
+        out->group_cap = best.group;
+        out->walk_warps = best.warps;
+        out->walk_stack = h->prm.walk_stack;
+        out->ms_force_phase = best_ms;
+        out->candidates = tried;
+    }
+    return NEXT_OK;
+}
+
+int next_get_params(const next_handle* h, next_params* p) {
+    if (!h || !p) return NEXT_ERR_INVALID_ARGUMENT;
+    *p = h->prm;
+    return NEXT_OK;
+}
+
 int next_flush_l2(next_handle* h) {
     if (!h) return NEXT_ERR_INVALID_ARGUMENT;
     if (!h->flush) {

@@ -89,7 +89,7 @@ __device__ __forceinline__ void pc_term(const float4* e, const Target& T, float 
     const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
     const float rinv = rsqrtf(r2);
     const float rinv2 = rinv * rinv;
-    const float mr3 = a.w * rinv * rinv2;
+    const float rinv3 = rinv2 * rinv;
     if (QUAD) {
         const float4 b = e[1];
         const float4 c = e[2];
@@ -97,14 +97,15 @@ __device__ __forceinline__ void pc_term(const float4* e, const Target& T, float 
         const float qdy = fmaf(c.y, dz, fmaf(b.y, dy, b.w * dx));
         const float qdz = fmaf(b.z, dz, fmaf(c.y, dy, c.x * dx));
         const float q = fmaf(dz, qdz, fmaf(dy, qdy, dx * qdx));
-        const float rinv5 = rinv2 * rinv2 * rinv;
-        const float c7 = 2.5f * q * (rinv5 * rinv2);
-        const float cc = mr3 + c7;
+        // G m / r^3 + 2.5 q / r^7 = (G m + 2.5 q / r^4) / r^3
+        const float cc = rinv3 * fmaf(q, (2.5f * rinv2) * rinv2, a.w);
+        const float rinv5 = rinv3 * rinv2;
         sx = fmaf(cc, dx, fmaf(-rinv5, qdx, sx));
         sy = fmaf(cc, dy, fmaf(-rinv5, qdy, sy));
         sz = fmaf(cc, dz, fmaf(-rinv5, qdz, sz));
         if (POT) sp = fmaf(-0.5f * q, rinv5, fmaf(-a.w, rinv, sp));
     } else {
+        const float mr3 = a.w * rinv3;
         sx = fmaf(mr3, dx, sx);
         sy = fmaf(mr3, dy, sy);
         sz = fmaf(mr3, dz, sz);
@@ -217,7 +218,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
     int* stack = reinterpret_cast<int*>(smem_raw + sizeof(WarpLists) * nwarps) + w * stack_cap;
     const uint32_t lt = (1u << lane) - 1u;
     const int64_t ngroups = t.counts[2];
-    const int64_t nnodes = t.counts[1];
+    const unsigned nnodes32 = static_cast<unsigned>(t.counts[1]);
+    const unsigned nbodies32 = static_cast<unsigned>(nbodies);
     unsigned long long npp = 0, npc = 0;
     int max_sp = 0;
 
@@ -275,12 +277,14 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             bool valid = node >= 0;
             float4 box = make_float4(0.f, 0.f, 0.f, -1.f);
             int2 lk = make_int2(0, 0);
-            if (valid && node >= nnodes) { raise_error(err, kErrIndex); valid = false; }
-            if (valid) { box = t.box[node]; lk = t.link[node]; valid = box.w >= 0.f; }
-            if (valid && (lk.y > 8 || lk.x < 0 || (lk.y > 0 && static_cast<int64_t>(lk.x) + lk.y > nnodes) ||
-                          (lk.y <= 0 && static_cast<int64_t>(lk.x) - lk.y > nbodies))) {
-                raise_error(err, kErrIndex);
-                valid = false;
+            if (valid) {
+                // index guard: the node, its children or its bodies must lie inside their arrays
+                const bool in_range = static_cast<unsigned>(node) < nnodes32;
+                if (in_range) { box = __ldg(t.box + node); lk = __ldg(t.link + node); }
+                const unsigned end = static_cast<unsigned>(lk.x) + static_cast<unsigned>(lk.y > 0 ? lk.y : -lk.y);
+                const bool bad = !in_range || lk.x < 0 || lk.y > 8 || end > (lk.y > 0 ? nnodes32 : nbodies32);
+                if (bad) raise_error(err, kErrIndex);
+                valid = !bad && box.w >= 0.f;
             }
             const float dx = fmaxf(fabsf(box.x - fgx) - hx, 0.f);
             const float dy = fmaxf(fabsf(box.y - fgy) - hy, 0.f);

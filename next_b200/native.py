@@ -25,6 +25,11 @@ class Params(C.Structure):
                 ("reuse_forces", C.c_int), ("walk_warps", C.c_int), ("walk_stack", C.c_int), ("device", C.c_int)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("leaf_cap", C.c_int), ("group_cap", C.c_int), ("walk_warps", C.c_int), ("walk_stack", C.c_int),
+                ("ms_force_phase", C.c_double), ("candidates", C.c_int)]
+
+
 class Stats(C.Structure):
     _fields_ = [("n_bodies", C.c_int64), ("n_systems", C.c_int64), ("n_nodes", C.c_int64),
                 ("n_internal", C.c_int64), ("n_groups", C.c_int64), ("pp_interactions", C.c_int64),
@@ -65,6 +70,8 @@ SIGNATURES = {
     "next_sort_pairs": (C.c_int, [_h, C.c_int64, _u64, _u32, _u64, _u32, C.c_int]),
     "next_fp32_peak": (C.c_int, [C.c_int, _d, _d]),
     "next_flush_l2": (C.c_int, [_h]),
+    "next_autotune": (C.c_int, [_h, C.POINTER(TuneResult)]),
+    "next_get_params": (C.c_int, [_h, C.POINTER(Params)]),
     "next_host_alloc": (C.c_void_p, [C.c_int64]),
     "next_host_free": (None, [C.c_void_p]),
     "next_kernel_launches": (C.c_int64, []),
@@ -220,6 +227,17 @@ class Simulation:
         s = Stats()
         self._check(self.lib.next_stats_get(self.h, C.byref(s)), "stats")
         return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def autotune(self):
+        r = TuneResult()
+        self._check(self.lib.next_autotune(self.h, C.byref(r)), "autotune")
+        self.params = self.get_params()
+        return {f: getattr(r, f) for f, _ in TuneResult._fields_}
+
+    def get_params(self):
+        p = Params()
+        self._check(self.lib.next_get_params(self.h, C.byref(p)), "get_params")
+        return p
 
     def set_timing(self, on: bool):
         self._check(self.lib.next_set_timing(self.h, int(bool(on))), "set_timing")

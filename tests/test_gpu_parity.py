@@ -302,3 +302,23 @@ def test_coincident_bodies_do_not_break_the_build():
         assert all(np.all(np.isfinite(a[c])) for c in a)
         assert sim.stats()["device_error"] == 0
         sim.close()
+
+
+def test_autotune_keeps_accuracy_and_state(oracle):
+    b = ic.uniform_sphere(65_536, seed=21)
+    sim = Simulation("accurate", "mixed", theta=0.5, eps=0.005)
+    sim.upload(b)
+    r = sim.autotune()
+    assert r["candidates"] >= 12 and r["leaf_cap"] <= r["group_cap"] <= 32
+    p = sim.get_params()
+    assert (p.leaf_cap, p.group_cap, p.walk_warps) == (r["leaf_cap"], r["group_cap"], r["walk_warps"])
+    s = sim.download()                       # tuning does not move bodies
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(s[c], b[c])
+    a = sim.accel()
+    idx = np.arange(0, 65_536, 64)
+    e = rel_err({c: a[c][idx] for c in a}, oracle.direct(b, idx, eps=0.005))
+    assert np.median(e) <= 1e-3
+    sim.step(5e-4)
+    assert sim.stats()["device_error"] == 0
+    sim.close()
