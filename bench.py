@@ -275,7 +275,10 @@ def run_ours(args):
         tdist.init_process_group("nccl", device_id=torch.device("cuda", local),
                                  timeout=__import__("datetime").timedelta(seconds=120))
         dist = tdist
-    W = CONFIGS[args.config]
+    W = dict(CONFIGS[args.config])
+    if args.n:
+        W["n"] = args.n
+        W["name"] = f"{W['name']}_n{args.n}"
     bodies, offsets = make_bodies(W)
     n = bodies["x"].shape[0]
     sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, leaf_cap=args.leaf_cap,
@@ -434,6 +437,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS), help="workload (default c2, the metric's)")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--n", type=int, default=None, help="override the body count of a single-system config")
     ap.add_argument("--leaf-cap", type=int, default=None, help="bodies per leaf of the mixed walk's tree")
     ap.add_argument("--group-cap", type=int, default=None, help="bodies per walk group (<= 32)")
     ap.add_argument("--walk-warps", type=int, default=None, help="warps per block of the mixed walk")
