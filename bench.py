@@ -280,12 +280,35 @@ def run_ours(args):
         W["n"] = args.n
         W["name"] = f"{W['name']}_n{args.n}"
     bodies, offsets = make_bodies(W)
+    sharded = world > 1 and offsets is None      # one system over all ranks (force all-gather)
+    if world > 1 and offsets is not None:
+        # independent systems: each rank integrates its own slice of them, no collective
+        s0 = rank * (len(offsets) - 1) // world
+        s1 = (rank + 1) * (len(offsets) - 1) // world
+        sl = slice(offsets[s0], offsets[s1])
+        bodies = {k: v[sl] for k, v in bodies.items()}
+        offsets = offsets[s0:s1 + 1] - offsets[s0]
     n = bodies["x"].shape[0]
-    sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, leaf_cap=args.leaf_cap,
-                     group_cap=args.group_cap, walk_warps=args.walk_warps, walk_stack=args.walk_stack)
+    knobs = dict(leaf_cap=args.leaf_cap, group_cap=args.group_cap, walk_warps=args.walk_warps,
+                 walk_stack=args.walk_stack)
+    sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, **knobs)
     sim.upload(bodies, offsets=offsets)
     sim.step(W["dt"])
     tune = None if args.no_autotune else sim.autotune()
+    if sharded:
+        # every rank must build the same tree: rank 0's tuned setting goes to all,
+        # and all ranks restart from the same initial bodies
+        from next_b200.dist import attach
+        import torch
+        p = sim.get_params()
+        t = torch.tensor([p.leaf_cap, p.group_cap, p.walk_warps, p.walk_stack], device=f"cuda:{local}")
+        dist.broadcast(t, src=0)
+        knobs = dict(zip(("leaf_cap", "group_cap", "walk_warps", "walk_stack"), (int(x) for x in t.tolist())))
+        sim.close()
+        sim = Simulation("accurate", "mixed", theta=W["theta"], eps=W["eps"], device=local, **knobs)
+        sim.upload(bodies)
+        attach(sim)
+        sim.step(W["dt"])
     # warm-up (capacities, force cache, clocks)
     for _ in range(args.warmup):
         sim.step(W["dt"])
@@ -325,13 +348,31 @@ def run_ours(args):
         t = torch.tensor([ms_total], device=f"cuda:{local}", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_total = float(t.item())
+    if dist:
+        import torch
+        tot = torch.tensor([float(st["pp_interactions"]), float(st["pc_interactions"]), st["ms_walk"]],
+                           device=f"cuda:{local}", dtype=torch.float64)
+        mx = tot[2:].clone()
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        st["pp_interactions"], st["pc_interactions"] = int(tot[0].item()), int(tot[1].item())
+        st["ms_walk"] = float(mx[0].item())
     clocks = clk.summary()
     diag1 = sim.diagnostics()
     e0 = diag0["kinetic"] + diag0["potential"]
     e1 = diag1["kinetic"] + diag1["potential"]
-    value = world * n * args.steps / (ms_total * 1e-3)
+    # sharded: every rank advances the same n bodies; independent systems: n is this rank's part
+    total_bodies = n if sharded else world * n if world > 1 else n
+    if world > 1 and not sharded:
+        import torch
+        tb = torch.tensor([float(n)], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tb, op=dist.ReduceOp.SUM)
+        total_bodies = int(tb.item())
+    value = total_bodies * args.steps / (ms_total * 1e-3)
     walk_ms = st["ms_walk"] / max(1, st["walk_launches"])
     flops_walk = (FLOPS_PP * st["pp_interactions"] + FLOPS_PC * st["pc_interactions"]) / max(1, st["walk_launches"])
+    if sharded:
+        flops_walk /= world          # per GPU: the interaction counts above are summed over ranks
     peak = fp32_peak(local)
     achieved = flops_walk / (walk_ms * 1e-3) / 1e12
     # ---- graph replay throughput of the same step (one captured graph per step)
@@ -345,7 +386,7 @@ def run_ours(args):
         fp64 = plain_fp64_leg(bodies, offsets, W, local, max(1, args.fp64_steps), idx)
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
-    if rank == 0 and not args.skip_e2e and offsets is None:
+    if rank == 0 and not args.skip_e2e and offsets is None and world == 1:
         import ctypes as C
         ptrs = [lib.next_host_alloc(8 * n) for _ in range(7)]
         lanes = [np.ctypeslib.as_array(C.cast(p_, C.POINTER(C.c_double)), shape=(n,)) for p_ in ptrs]
@@ -382,22 +423,24 @@ def run_ours(args):
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 interactions / f64 state", "data": "synthetic",
+        "scaling": "strong" if sharded else "weak", "vs_baseline": None, "dtype": "f32 interactions / f64 state",
+        "data": "synthetic",
         "config": {"workload": W["name"], "n_bodies": n, "n_systems": 1 if offsets is None else len(offsets) - 1,
                    "theta": W["theta"], "eps": W["eps"], "dt": W["dt"], "seed": W["seed"],
                    "physics": "accurate (Plummer eps, full-width theta, corrected quadrupole)",
                    "precision": "FP32-mixed", "leaf_cap": prm.leaf_cap, "group_cap": prm.group_cap,
                    "walk_warps": prm.walk_warps, "walk_stack": prm.walk_stack,
                    "autotuned": tune is not None,
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "parallelism": (f"sharded x{world}: force walk split by body share, NCCL all-gather of forces"
+                                   if sharded else f"{world} ranks x independent systems" if world > 1 else "1 GPU"),
                    "l2": "flushed between steps (256 MiB write outside the timed events); step working set > L2"},
         "force_error": {"mixed": err_mixed, "fp64_plain": fp64["force_error"] if fp64 else None,
                         "versus": "FP64 direct summation on seeded bodies"},
         "fp64_gpu": fp64,
-        "speedup_vs_fp64_gpu": (value / world) / fp64["value"] if fp64 else None,
+        "speedup_vs_fp64_gpu": value / fp64["value"] if fp64 and world == 1 else None,
         "graph_value": n * args.steps / graph_s,
         "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
-        "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / n,
+        "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / total_bodies,
         "pp_fraction": st["pp_interactions"] / max(1, st["pp_interactions"] + st["pc_interactions"]),
         "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - st["n_systems"],
                  "bodies_per_group": n / max(1, st["n_groups"] - st["n_systems"]), "max_walk_stack": st["max_stack"]},

@@ -225,6 +225,24 @@ int next_autotune(next_handle* h, next_tune_result* out);
 /* The handle's current parameters (after autotuning or capacity growth). */
 int next_get_params(const next_handle* h, next_params* p);
 
+/* Sharding one system over several GPUs (one process and one handle per
+ * GPU).  Every rank uploads the same bodies and keeps all of them; each builds
+ * the full tree (identical on every rank), walks only its share of the bodies
+ * (working positions [rank*c, (rank+1)*c), c = ceil(n/world)), and the forces
+ * are completed with in-place NCCL all-gathers over NVLink (24 B per body per
+ * force phase), so kick and drift stay bit-identical on all ranks.  This
+ * replaces the reference's replicated-data MPI decomposition
+ * (src/gravity/step.h:36-65, 125-188: slice [rank*N/size, (rank+1)*N/size),
+ * MPI_Allreduce of the box, MPI_Iallgatherv of v and x).
+ *   next_dist_unique_id: rank 0 makes the 128-byte NCCL id; the caller sends
+ *     it to the other ranks (e.g. over its own process group).
+ *   next_dist_attach: joins the communicator (blocks until all ranks join).
+ *     With id128 == NULL no communicator is made and the handle computes only
+ *     its own share (one-device emulation of a rank, for tests).
+ * NCCL is loaded at run time (libnccl.so.2). */
+int next_dist_unique_id(unsigned char* id128);
+int next_dist_attach(next_handle* h, int rank, int world, const unsigned char* id128);
+
 /* Page-locked host memory for body arrays, so uploads and downloads run at
  * full PCIe/C2C bandwidth.  Free with next_host_free. */
 void* next_host_alloc(int64_t bytes);

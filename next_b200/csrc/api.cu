@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "dist.cuh"
 #include "kernels.cuh"
 
 using namespace nb;
@@ -135,6 +136,11 @@ struct next_handle {
     bool pot_valid = false;
     bool sorted_in_alt = false;
 
+    // sharding over ranks: every rank holds all bodies, computes the forces of
+    // its share [rank*chunk, (rank+1)*chunk) and all-gathers the rest
+    int world = 1, rank = 0;
+    void* comm = nullptr;
+
     // graphs: one captured KDK step per buffer parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t graph_kernels[2] = {0, 0};
@@ -218,6 +224,18 @@ int64_t initial_cap_int(const next_handle* h) {
     return h->cap_n / leaf + h->cap_n / (4 * leaf) + 1024;
 }
 
+// This rank's share of the bodies (working positions) for the force walk.
+void set_share(next_handle* h) {
+    if (h->world <= 1) {
+        h->P.own_lo = 0;
+        h->P.own_hi = INT64_MAX;
+        return;
+    }
+    const int64_t chunk = (h->n + h->world - 1) / h->world;
+    h->P.own_lo = std::min<int64_t>(h->n, h->rank * chunk);
+    h->P.own_hi = std::min<int64_t>(h->n, h->P.own_lo + chunk);
+}
+
 void free_bodies(next_handle* h) {
     drop_graphs(h);
     for (auto& b : h->buf) b.free_all();
@@ -237,7 +255,8 @@ int alloc_bodies(next_handle* h, int64_t n) {
     h->buf[0].alloc_all(n, e);
     h->buf[1].alloc_all(n, e);
     auto A = [&](auto** p, size_t c) { if (e == cudaSuccess) e = dalloc(p, c); };
-    A(&h->ax, n); A(&h->ay, n); A(&h->az, n); A(&h->pot, n);
+    const int64_t padded = ((n + h->world - 1) / h->world) * h->world;   // world equal shares
+    A(&h->ax, padded); A(&h->ay, padded); A(&h->az, padded); A(&h->pot, padded);
     A(&h->keys, n); A(&h->keys_alt, n); A(&h->idx, n); A(&h->idx_alt, n); A(&h->inv, n);
     A(&h->sysid, n); A(&h->d_offsets, h->nsys + 1); A(&h->cubes, h->nsys);
     h->sort_words = sort_scratch_words(n);
@@ -309,10 +328,24 @@ int walk(next_handle* h, bool potential) {
     return NEXT_OK;
 }
 
+int exchange_forces(next_handle* h, bool potential) {
+    if (h->world <= 1 || !h->comm) return NEXT_OK;
+    const size_t chunk = static_cast<size_t>((h->n + h->world - 1) / h->world);
+    double* lanes[4] = {h->ax, h->ay, h->az, h->pot};
+    std::string why;
+    for (int c = 0; c < (potential ? 4 : 3); ++c)
+        if (!nccl_allgather_inplace(h->comm, lanes[c], chunk, h->rank, h->st, &why))
+            return fail(h, NEXT_ERR_CUDA, why);
+    count_launches(potential ? 4 : 3);
+    return NEXT_OK;
+}
+
 int forces(next_handle* h, bool potential, std::vector<int>* evs) {
     int rc = build(h, evs);
     if (rc) return rc;
     rc = walk(h, potential);
+    if (rc) return rc;
+    rc = exchange_forces(h, potential);
     if (rc) return rc;
     h->forces_valid = true;
     h->pot_valid = potential;
@@ -579,6 +612,9 @@ void next_destroy(next_handle* h) {
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->st) cudaStreamSynchronize(h->st);
+    drop_graphs(h);
+    nccl_comm_destroy(h->comm);
+    h->comm = nullptr;
     free_bodies(h);
     dfree(h->err); dfree(h->stats); dfree(h->queue); dfree(h->tickets); dfree(h->partial);
     dfree(h->dts); dfree(h->dt_out); dfree(h->diag); dfree(h->changed); dfree(h->fma_out); dfree(h->t.counts);
@@ -635,6 +671,7 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
         }
         S.offsets = h->d_offsets;
         S.cube = h->cubes;
+        set_share(h);
         NB_TRY(cudaMemcpyAsync(h->d_offsets, offsets, sizeof(int64_t) * (n_systems + 1), cudaMemcpyHostToDevice, h->st),
                "offsets");
         std::vector<int32_t> sid(n);
@@ -1117,6 +1154,41 @@ int next_autotune(next_handle* h, next_tune_result* out) {
 int next_get_params(const next_handle* h, next_params* p) {
     if (!h || !p) return NEXT_ERR_INVALID_ARGUMENT;
     *p = h->prm;
+    return NEXT_OK;
+}
+
+int next_dist_unique_id(unsigned char* id128) {
+    if (!id128) return NEXT_ERR_INVALID_ARGUMENT;
+    std::string why;
+    return nccl_unique_id(id128, &why) ? NEXT_OK : NEXT_ERR_CUDA;
+}
+
+int next_dist_attach(next_handle* h, int rank, int world, const unsigned char* id128) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (world < 1 || rank < 0 || rank >= world) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad rank/world");
+    if (h->nsys > 1) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "sharding applies to a single system");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "set device");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    drop_graphs(h);
+    nccl_comm_destroy(h->comm);
+    h->comm = nullptr;
+    if (world > 1 && id128) {
+        std::string why;
+        if (!nccl_comm_init(&h->comm, rank, world, id128, &why)) return fail(h, NEXT_ERR_CUDA, why);
+    }
+    const bool resize = h->have_bodies && world != h->world;
+    h->world = world;
+    h->rank = rank;
+    if (resize) {
+        dfree(h->ax); dfree(h->ay); dfree(h->az); dfree(h->pot);
+        const int64_t padded = ((h->cap_n + world - 1) / world) * world;
+        auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
+        A(&h->ax, padded); A(&h->ay, padded); A(&h->az, padded); A(&h->pot, padded);
+        if (e != cudaSuccess) return cuda_fail(h, e, "force arrays");
+    }
+    set_share(h);
+    h->forces_valid = false;
     return NEXT_OK;
 }
 

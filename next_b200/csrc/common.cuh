@@ -71,6 +71,9 @@ struct Params {
     int physics;           // NEXT_PHYSICS_*
     double theta, eps, G;
     int leaf_cap, group_cap, quad;
+    // bodies (working positions) whose forces this device computes; the
+    // whole range on one device, one share of it per rank when sharded
+    int64_t own_lo = 0, own_hi = INT64_MAX;
 };
 
 // Key layout: the system number sits in bits [base, 63), the octant digit of

@@ -209,7 +209,7 @@ __device__ __forceinline__ void eval_pp(WarpLists& L, const int* list, int count
 template <bool QUAD, bool SOFT, bool POT>
 __global__ void __launch_bounds__(128, NB_WALK_MIN_BLOCKS)
 walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int stack_cap, unsigned int* queue,
-                  unsigned long long* stats, int* err) {
+                  unsigned long long* stats, int* err, int64_t own_lo, int64_t own_hi) {
     if (*err & kErrAbort) return;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -235,6 +235,11 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrIndex);
             continue;
         }
+        // sharded: only groups that hold bodies of this device's share
+        if (static_cast<int64_t>(grp.x) + nt <= own_lo || grp.x >= own_hi) continue;
+        const int64_t own_first = grp.x > own_lo ? grp.x : own_lo;
+        const int64_t own_end = static_cast<int64_t>(grp.x) + nt < own_hi ? static_cast<int64_t>(grp.x) + nt : own_hi;
+        const unsigned long long own_nt = static_cast<unsigned long long>(own_end - own_first);
         // Groups of at most 16 bodies are evaluated by 2, 4, ... warp slices,
         // each taking a share of every list batch; slices are summed at the end.
         int nslices = 1;
@@ -358,14 +363,14 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             fz += __shfl_xor_sync(0xffffffffu, fz, o);
             if (POT) fp += __shfl_xor_sync(0xffffffffu, fp, o);
         }
-        if (active && slice == 0) {
+        if (active && slice == 0 && i >= own_lo && i < own_hi) {
             bd.ax[i] = fx;
             bd.ay[i] = fy;
             bd.az[i] = fz;
             if (POT && bd.pot) bd.pot[i] = fp;
         }
-        npp += g_pp * static_cast<unsigned long long>(nt);
-        npc += g_pc * static_cast<unsigned long long>(nt);
+        npp += g_pp * own_nt;
+        npc += g_pc * own_nt;
     }
     if (lane == 0) {
         if (npp) atomicAdd(stats + 0, npp);
@@ -389,7 +394,8 @@ cudaError_t launch_variant(const Bodies& bd, int64_t nbodies, const Tree& t, con
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
     kern<<<per_sm * sm_count, 32 * warps, smem, st>>>(bd, nbodies, t, static_cast<float>(P.G),
-                                                     static_cast<float>(P.eps * P.eps), stack_cap, queue, stats, err);
+                                                     static_cast<float>(P.eps * P.eps), stack_cap, queue, stats, err,
+                                                     P.own_lo, P.own_hi);
     count_launches(1);
     return cudaGetLastError();
 }

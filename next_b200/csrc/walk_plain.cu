@@ -73,7 +73,7 @@ walk_plain_kernel(Bodies bd, const int32_t* __restrict__ sysid, int64_t n, Tree 
     if (*err & kErrAbort) return;
     const int64_t nodes = t.counts[1];
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool active = i < n;
+    const bool active = i < n && i >= P.own_lo && i < P.own_hi;
     unsigned long long npp = 0, npc = 0;
     if (active) {
         const int root = sysid ? sysid[i] : 0;

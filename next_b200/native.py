@@ -72,6 +72,8 @@ SIGNATURES = {
     "next_flush_l2": (C.c_int, [_h]),
     "next_autotune": (C.c_int, [_h, C.POINTER(TuneResult)]),
     "next_get_params": (C.c_int, [_h, C.POINTER(Params)]),
+    "next_dist_unique_id": (C.c_int, [C.c_void_p]),
+    "next_dist_attach": (C.c_int, [_h, C.c_int, C.c_int, C.c_void_p]),
     "next_host_alloc": (C.c_void_p, [C.c_int64]),
     "next_host_free": (None, [C.c_void_p]),
     "next_kernel_launches": (C.c_int64, []),
@@ -101,6 +103,16 @@ def load(path: str = LIB_PATH):
 
 class NextError(RuntimeError):
     pass
+
+
+def dist_unique_id() -> bytes:
+    """A fresh 128-byte NCCL unique id (made by rank 0 of a sharded run)."""
+    lib = load()
+    buf = C.create_string_buffer(128)
+    rc = lib.next_dist_unique_id(buf)
+    if rc:
+        raise NextError(f"next_dist_unique_id failed ({rc})")
+    return buf.raw
 
 
 def _p(a, t):
@@ -238,6 +250,11 @@ class Simulation:
         p = Params()
         self._check(self.lib.next_get_params(self.h, C.byref(p)), "get_params")
         return p
+
+    def dist_attach(self, rank: int, world: int, unique_id: bytes | None):
+        """Join a sharded run (unique_id from dist_unique_id on rank 0); None: own share only."""
+        buf = None if unique_id is None else C.create_string_buffer(bytes(unique_id), 128)
+        self._check(self.lib.next_dist_attach(self.h, int(rank), int(world), buf), "dist_attach")
 
     def set_timing(self, on: bool):
         self._check(self.lib.next_set_timing(self.h, int(bool(on))), "set_timing")

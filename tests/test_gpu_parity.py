@@ -322,3 +322,35 @@ def test_autotune_keeps_accuracy_and_state(oracle):
     sim.step(5e-4)
     assert sim.stats()["device_error"] == 0
     sim.close()
+
+
+@pytest.mark.parametrize("precision,world", [("mixed", 2), ("mixed", 3), ("fp64", 2)])
+def test_sharded_shares_equal_single_device(precision, world):
+    """Each rank walks only its share of the bodies (key order); stitched, the
+    shares equal the one-device forces bit for bit.  Ranks are emulated on one
+    device (no communicator: next_dist_attach with id NULL)."""
+    from next_b200.dist import partition
+    b = ic.plummer(50_000, seed=31)
+    leaf = 16 if precision == "mixed" else 1
+    full = Simulation("accurate", precision, leaf_cap=leaf)
+    full.upload(b)
+    want = full.accel()
+    order = full.debug_order()
+    got = {c: np.full(50_000, np.nan) for c in ("ax", "ay", "az")}
+    total_pc = 0
+    for r in range(world):
+        s = Simulation("accurate", precision, leaf_cap=leaf)
+        s.upload(b)
+        s.dist_attach(r, world, None)
+        a = s.accel()
+        np.testing.assert_array_equal(s.debug_order(), order)     # identical trees on every rank
+        lo, hi, _ = partition(50_000, world, r)
+        mine = order[lo:hi]
+        for c in got:
+            got[c][mine] = a[c][mine]
+        total_pc += s.stats()["pc_interactions"]
+        s.close()
+    for c in got:
+        np.testing.assert_array_equal(got[c], want[c])
+    assert total_pc == full.stats()["pc_interactions"]
+    full.close()
