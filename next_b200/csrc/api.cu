@@ -115,6 +115,7 @@ struct next_handle {
     // pinned host scalars
     double* h_dts = nullptr;
     int* h_err = nullptr;
+    int* h_flags = nullptr;                // upload check: changed, non-finite, negative mass
     int64_t* h_counts = nullptr;           // internal, nodes, groups
     unsigned long long* h_stats = nullptr;
 
@@ -144,6 +145,11 @@ struct next_handle {
     // graphs: one captured KDK step per buffer parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t graph_kernels[2] = {0, 0};
+    // events recorded inside each graph (build start, after keys, after sort,
+    // after build, after walk) so a timed replay reports its stages
+    std::vector<cudaEvent_t> graph_ev[2];
+    std::vector<cudaEvent_t> cap_events;
+    bool capturing = false;
 
     // timing
     bool timing = false;
@@ -188,8 +194,11 @@ void free_tree(next_handle* h) {
 }
 
 void drop_graphs(next_handle* h) {
-    for (auto& g : h->graph)
-        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    for (int p = 0; p < 2; ++p) {
+        if (h->graph[p]) { cudaGraphExecDestroy(h->graph[p]); h->graph[p] = nullptr; }
+        for (cudaEvent_t ev : h->graph_ev[p]) cudaEventDestroy(ev);
+        h->graph_ev[p].clear();
+    }
 }
 
 int alloc_tree(next_handle* h, int64_t cap_int) {
@@ -267,16 +276,20 @@ int alloc_bodies(next_handle* h, int64_t n) {
     return alloc_tree(h, initial_cap_int(h));
 }
 
-bool finite_array(const double* a, int64_t n) {
-    for (int64_t i = 0; i < n; ++i)
-        if (!std::isfinite(a[i])) return false;
-    return true;
-}
 
 // ---- the force phase -------------------------------------------------------
 
 int record(next_handle* h, std::vector<int>* evs) {
     if (!evs) return NEXT_OK;
+    if (h->capturing) {
+        // inside a capture: a dedicated event becomes an event-record node of
+        // the graph (External, so replays really record it)
+        cudaEvent_t ev;
+        NB_TRY(cudaEventCreate(&ev), "event create");
+        NB_TRY(cudaEventRecordWithFlags(ev, h->st, cudaEventRecordExternal), "event record");
+        h->cap_events.push_back(ev);
+        return NEXT_OK;
+    }
     if (h->ev_used >= h->ev_pool.size()) {
         cudaEvent_t ev;
         NB_TRY(cudaEventCreate(&ev), "event create");
@@ -449,8 +462,14 @@ int capture_step(next_handle* h) {
     NB_TRY(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed), "begin capture");
     int rc = NEXT_OK;
     Bodies bd = h->cur_bodies();
+    h->capturing = true;
+    h->cap_events.clear();
+    std::vector<int> unused;
     cudaError_t e = launch_kick_drift(bd, h->n, h->dts, h->err, h->st);
-    if (e == cudaSuccess) rc = forces(h, false, nullptr);
+    if (e == cudaSuccess) rc = forces(h, false, &unused);
+    h->capturing = false;
+    h->graph_ev[parity] = h->cap_events;
+    h->cap_events.clear();
     if (e == cudaSuccess && rc == NEXT_OK) {
         bd = h->cur_bodies();
         e = launch_kick(bd, h->n, h->dts, h->err, h->st);
@@ -498,6 +517,34 @@ int resolve_timers(next_handle* h) {
         h->timed_walks += 1;
     }
     h->ev_steps.clear();
+    h->ev_used = 0;
+    return NEXT_OK;
+}
+
+// One timed graph replay: step = the events around the launch; stages from
+// the events recorded inside the graph.
+int add_graph_timing(next_handle* h, int parity, const std::vector<int>& evs) {
+    const std::vector<cudaEvent_t>& g = h->graph_ev[parity];
+    if (evs.size() != 2 || g.size() != 5) return NEXT_OK;
+    bool ok = true;
+    auto el = [&ok](cudaEvent_t a, cudaEvent_t b) {
+        float v = 0.f;
+        if (cudaEventElapsedTime(&v, a, b) != cudaSuccess) ok = false;
+        return static_cast<double>(v);
+    };
+    const double step = el(h->ev_pool[evs[0]], h->ev_pool[evs[1]]);
+    const double build = el(g[0], g[3]), walkms = el(g[3], g[4]), sortms = el(g[1], g[2]);
+    if (!ok) {
+        cudaGetLastError();   // do not let a timing failure surface as a later launch error
+        return fail(h, NEXT_ERR_CUDA, "stage timing of a graph replay failed");
+    }
+    h->acc_step += step;
+    h->acc_build += build;
+    h->acc_walk += walkms;
+    h->acc_sort += sortms;
+    h->acc_other += step - build - walkms;
+    h->timed_steps += 1;
+    h->timed_walks += 1;
     h->ev_used = 0;
     return NEXT_OK;
 }
@@ -592,7 +639,7 @@ int next_create(const next_params* p, next_handle** out) {
     if (e != cudaSuccess) return bail(e, "sort setup");
     auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
     A(&h->err, 1); A(&h->stats, 4); A(&h->queue, 1); A(&h->tickets, 4); A(&h->partial, kReduceMax * 8);
-    A(&h->dts, 2); A(&h->dt_out, 2); A(&h->diag, 8); A(&h->changed, 1); A(&h->fma_out, 1);
+    A(&h->dts, 2); A(&h->dt_out, 2); A(&h->diag, 8); A(&h->changed, 4); A(&h->fma_out, 1);
     A(&h->t.counts, 4);
     if (e != cudaSuccess) return bail(e, "scalars");
     e = cudaMemset(h->err, 0, sizeof(int));
@@ -601,6 +648,7 @@ int next_create(const next_params* p, next_handle** out) {
     if (e == cudaSuccess) e = cudaMemset(h->t.counts, 0, sizeof(int64_t) * 4);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_dts), sizeof(double) * 2, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_err), sizeof(int) * 2, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_flags), sizeof(int) * 4, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_counts), sizeof(int64_t) * 4, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_stats), sizeof(unsigned long long) * 4, cudaHostAllocDefault);
     if (e != cudaSuccess) return bail(e, "pinned scalars");
@@ -623,6 +671,7 @@ void next_destroy(next_handle* h) {
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
     if (h->h_dts) cudaFreeHost(h->h_dts);
     if (h->h_err) cudaFreeHost(h->h_err);
+    if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->h_counts) cudaFreeHost(h->h_counts);
     if (h->h_stats) cudaFreeHost(h->h_stats);
     if (h->st) cudaStreamDestroy(h->st);
@@ -642,10 +691,6 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
     if (n < 1 || n >= (int64_t(1) << 30))
         return fail(h, NEXT_ERR_INVALID_ARGUMENT, "body count must be in [1, 2^30)");
     if (!x || !y || !z || !vx || !vy || !vz || !m) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "NULL body array");
-    for (const double* a : {x, y, z, vx, vy, vz, m})
-        if (!finite_array(a, n)) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "non-finite body data");
-    for (int64_t i = 0; i < n; ++i)
-        if (m[i] < 0.0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "negative mass");
     cudaError_t e = cudaSetDevice(h->device);
     if (e != cudaSuccess) return cuda_fail(h, e, "set device");
     const bool same_layout = h->have_bodies && h->n == n && h->nsys == n_systems &&
@@ -688,16 +733,19 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
     } else {
         NB_TRY(cudaMemsetAsync(h->stype, 0, sizeof(int) * n, h->st), "types");
     }
+    // validate on the device (finite values, m >= 0) and, for the same layout,
+    // find out whether positions/masses/types changed; the held bodies are
+    // only touched once the staged data passed
     Bodies b = h->cur_bodies();
-    if (same_layout) {
-        NB_TRY(cudaMemsetAsync(h->changed, 0, sizeof(int), h->st), "compare flag");
-        NB_TRY(launch_compare(h->stage, h->stype, b, h->inv, n, h->changed, h->st), "compare");
-        NB_TRY(cudaMemcpyAsync(h->h_err + 1, h->changed, sizeof(int), cudaMemcpyDeviceToHost, h->st), "compare flag");
-        NB_TRY(cudaStreamSynchronize(h->st), "sync");
-        if (h->h_err[1] == 0) {
-            NB_TRY(launch_load_velocities(h->stage, b, h->inv, n, h->st), "velocities");
-            return NEXT_OK;   // same positions: tree order and cached forces stay valid
-        }
+    NB_TRY(cudaMemsetAsync(h->changed, 0, sizeof(int) * 3, h->st), "upload flags");
+    NB_TRY(launch_check_upload(h->stage, h->stype, b, h->inv, n, same_layout, h->changed, h->st), "upload check");
+    NB_TRY(cudaMemcpyAsync(h->h_flags, h->changed, sizeof(int) * 3, cudaMemcpyDeviceToHost, h->st), "upload flags");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    if (h->h_flags[1]) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "non-finite body data");
+    if (h->h_flags[2]) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "negative mass");
+    if (same_layout && h->h_flags[0] == 0) {
+        NB_TRY(launch_load_velocities(h->stage, b, h->inv, n, h->st), "velocities");
+        return NEXT_OK;   // same positions: tree order and cached forces stay valid
     }
     NB_TRY(launch_load_all(h->stage, h->stype, b, h->inv, n, h->st), "load");
     h->forces_valid = false;
@@ -747,7 +795,7 @@ int next_steps(next_handle* h, double dt, int nsteps) {
     if (!std::isfinite(dt) || nsteps < 0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad dt or step count");
     rc = set_dt(h, dt);
     if (rc) return rc;
-    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces && !h->timing;
+    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces;
     int done = 0;
     while (done < nsteps) {
         if (!use_graph || !h->forces_valid) {
@@ -767,8 +815,24 @@ int next_steps(next_handle* h, double dt, int nsteps) {
         }
         rc = capture_step(h);
         if (rc) return rc;
-        NB_TRY(cudaGraphLaunch(h->graph[h->cur], h->st), "graph launch");
-        count_launches(static_cast<int>(h->graph_kernels[h->cur]));
+        const int parity = h->cur;
+        std::vector<int> evs;
+        if (h->timing) {
+            rc = resolve_timers(h);   // eager steps timed earlier keep their pool events until read
+            if (rc) return rc;
+            rc = record(h, &evs);
+            if (rc) return rc;
+        }
+        NB_TRY(cudaGraphLaunch(h->graph[parity], h->st), "graph launch");
+        count_launches(static_cast<int>(h->graph_kernels[parity]));
+        if (h->timing) {
+            // stage times of this replay: its in-graph events are overwritten by the next one
+            rc = record(h, &evs);
+            if (rc) return rc;
+            NB_TRY(cudaStreamSynchronize(h->st), "sync");
+            rc = add_graph_timing(h, parity, evs);
+            if (rc) return rc;
+        }
         h->cur = 1 - h->cur;
         ++done;
         if (done == nsteps || (done & 63) == 0) {

@@ -130,16 +130,24 @@ diagnostics_kernel(Bodies b, int64_t n, bool have_pot, double* partial, unsigned
     *ticket = 0u;
 }
 
-// Upload support: did positions, masses or types change?  Compared through
-// inv (caller index -> working position).
-__global__ void compare_kernel(const double* __restrict__ stage, const int* __restrict__ stype, Bodies b,
-                               const uint32_t* __restrict__ inv, int64_t n, int* changed) {
+// Upload support, one pass over the staged lanes: flags[1] = a non-finite
+// value, flags[2] = a negative mass, and (compare) flags[0] = positions,
+// masses or types differ from the bodies the handle holds (compared through
+// inv: caller index -> working position).
+__global__ void check_upload_kernel(const double* __restrict__ stage, const int* __restrict__ stype, Bodies b,
+                                    const uint32_t* __restrict__ inv, int64_t n, bool compare, int* flags) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t p = inv[i];
-    const bool same = stage[i] == b.x[p] && stage[n + i] == b.y[p] && stage[2 * n + i] == b.z[p] &&
-                      stage[6 * n + i] == b.m[p] && stype[i] == b.type[p];
-    if (!same) *changed = 1;
+    bool finite = true;
+    for (int c = 0; c < 7; ++c) finite &= isfinite(stage[c * n + i]);
+    if (!finite) flags[1] = 1;
+    if (stage[6 * n + i] < 0.0) flags[2] = 1;
+    if (compare) {
+        const uint32_t p = inv[i];
+        const bool same = stage[i] == b.x[p] && stage[n + i] == b.y[p] && stage[2 * n + i] == b.z[p] &&
+                          stage[6 * n + i] == b.m[p] && stype[i] == b.type[p];
+        if (!same) flags[0] = 1;
+    }
 }
 
 __global__ void load_velocities_kernel(const double* __restrict__ stage, Bodies b, const uint32_t* __restrict__ inv,
@@ -245,10 +253,10 @@ cudaError_t launch_diagnostics(const Bodies& b, int64_t n, bool have_pot, double
     return cudaGetLastError();
 }
 
-cudaError_t launch_compare(const double* stage, const int* stype, const Bodies& b, const uint32_t* inv, int64_t n,
-                           int* changed, cudaStream_t st) {
+cudaError_t launch_check_upload(const double* stage, const int* stype, const Bodies& b, const uint32_t* inv, int64_t n,
+                                bool compare, int* flags, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    compare_kernel<<<grid_for(n, 256), 256, 0, st>>>(stage, stype, b, inv, n, changed);
+    check_upload_kernel<<<grid_for(n, 256), 256, 0, st>>>(stage, stype, b, inv, n, compare, flags);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -63,8 +63,8 @@ cudaError_t launch_adaptive_dt(const Bodies& b, int64_t n, double base_dt, doubl
                                double* out, cudaStream_t st);
 cudaError_t launch_diagnostics(const Bodies& b, int64_t n, bool have_pot, double* partial, unsigned int* ticket,
                                double* out, cudaStream_t st);
-cudaError_t launch_compare(const double* stage, const int* stype, const Bodies& b, const uint32_t* inv, int64_t n,
-                           int* changed, cudaStream_t st);
+cudaError_t launch_check_upload(const double* stage, const int* stype, const Bodies& b, const uint32_t* inv, int64_t n,
+                                bool compare, int* flags, cudaStream_t st);
 cudaError_t launch_load_velocities(const double* stage, const Bodies& b, const uint32_t* inv, int64_t n,
                                    cudaStream_t st);
 cudaError_t launch_load_all(const double* stage, const int* stype, const Bodies& b, uint32_t* inv, int64_t n,

@@ -354,3 +354,20 @@ def test_sharded_shares_equal_single_device(precision, world):
         np.testing.assert_array_equal(got[c], want[c])
     assert total_pc == full.stats()["pc_interactions"]
     full.close()
+
+
+def test_timed_graph_replays_report_stages():
+    b = ic.plummer(40_000, seed=41)
+    sim = Simulation("accurate", "mixed")
+    sim.upload(b)
+    sim.step(1e-3)
+    sim.reset_timers()
+    sim.set_timing(True)
+    sim.steps(1e-3, 5)
+    sim.set_timing(False)
+    st = sim.stats()
+    assert st["steps"] == 5 and st["walk_launches"] == 5
+    assert st["ms_walk"] > 0 and st["ms_build"] > 0 and st["ms_sort"] > 0
+    assert st["ms_step"] >= st["ms_walk"] + st["ms_build"] - 1e-3
+    assert st["pc_interactions"] > 0 and st["device_error"] == 0
+    sim.close()
