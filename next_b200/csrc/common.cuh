@@ -60,7 +60,7 @@ struct Tree {
     double4* com;          // FP64 centre of mass and mass
     double* quad64;        // 8 per node: Qxx Qyy Qzz Qxy Qxz Qyz half-width rcrit
     float4* box;           // FP32 COM and rcrit^2 (mixed walk traversal)
-    float4* quad32;        // 2 per node: (Qxx Qyy Qzz Qxy) (Qxz Qyz 0 0), G folded in
+    float4* quad32;        // 2 per node: -G (Qxx Qyy Qzz Qxy) (Qxz Qyz 0 0)
     // walk groups
     int4* groups;          // (first body, count, root node, 0)
     // device scalars: [0] internal count, [1] node count, [2] group count

@@ -235,11 +235,12 @@ __device__ __forceinline__ void store_moments(Tree& t, int nid, const Mom& a, do
     if (accurate) {
         const float r2 = a.m > 0.0 ? static_cast<float>(rcrit * rcrit) : -1.0f;
         t.box[nid] = make_float4(static_cast<float>(a.cx), static_cast<float>(a.cy), static_cast<float>(a.cz), r2);
+        // stored negated (-G Q): the walk's quadrupole terms then need no negation
         t.quad32[2 * static_cast<int64_t>(nid)] =
-            make_float4(static_cast<float>(G * a.q[0]), static_cast<float>(G * a.q[1]),
-                        static_cast<float>(G * a.q[2]), static_cast<float>(G * a.q[3]));
+            make_float4(static_cast<float>(-G * a.q[0]), static_cast<float>(-G * a.q[1]),
+                        static_cast<float>(-G * a.q[2]), static_cast<float>(-G * a.q[3]));
         t.quad32[2 * static_cast<int64_t>(nid) + 1] =
-            make_float4(static_cast<float>(G * a.q[4]), static_cast<float>(G * a.q[5]), 0.0f, 0.0f);
+            make_float4(static_cast<float>(-G * a.q[4]), static_cast<float>(-G * a.q[5]), 0.0f, 0.0f);
     }
 }
 

@@ -31,13 +31,16 @@ namespace {
 // Compile-time knobs of the evaluation loop (unroll depth of a full batch and
 // the minimum resident blocks the register allocation must allow).
 #ifndef NB_WALK_UNROLL
-#define NB_WALK_UNROLL 8
+#define NB_WALK_UNROLL 4
 #endif
 #ifndef NB_WALK_GENERIC_UNROLL
 #define NB_WALK_GENERIC_UNROLL 1
 #endif
 #ifndef NB_WALK_FIXED
 #define NB_WALK_FIXED 1
+#endif
+#ifndef NB_WALK_PACKED
+#define NB_WALK_PACKED 1
 #endif
 #ifndef NB_WALK_MIN_BLOCKS
 #define NB_WALK_MIN_BLOCKS 6
@@ -79,8 +82,10 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
 }
 
 // One body-cell interaction (monopole + traceless quadrupole) from a staged
-// entry e[0] = (dx, dy, dz, G m) relative to the group centre, e[1] = G (Qxx Qyy
-// Qzz Qxy), e[2] = G (Qxz Qyz - -).  56 algorithmic flops.
+// entry e[0] = (dx, dy, dz, G m) relative to the group centre, e[1] = -G (Qxx
+// Qyy Qzz Qxy), e[2] = -G (Qxz Qyz - -).  56 algorithmic flops.  With the
+// negated Q, qd = -Q d and q = -d.Q.d, so
+//   a = (G m + 2.5 q_true / r^4) / r^3 d - Q d / r^5 = rinv3 (G m - 2.5 q rinv4) d + rinv5 qd.
 template <bool QUAD, bool POT>
 __device__ __forceinline__ void pc_term(const float4* e, const Target& T, float eps2, float& sx, float& sy,
                                         float& sz, float& sp) {
@@ -97,13 +102,12 @@ __device__ __forceinline__ void pc_term(const float4* e, const Target& T, float 
         const float qdy = fmaf(c.y, dz, fmaf(b.y, dy, b.w * dx));
         const float qdz = fmaf(b.z, dz, fmaf(c.y, dy, c.x * dx));
         const float q = fmaf(dz, qdz, fmaf(dy, qdy, dx * qdx));
-        // G m / r^3 + 2.5 q / r^7 = (G m + 2.5 q / r^4) / r^3
-        const float cc = rinv3 * fmaf(q, (2.5f * rinv2) * rinv2, a.w);
+        const float cc = rinv3 * fmaf(q, (-2.5f * rinv2) * rinv2, a.w);
         const float rinv5 = rinv3 * rinv2;
-        sx = fmaf(cc, dx, fmaf(-rinv5, qdx, sx));
-        sy = fmaf(cc, dy, fmaf(-rinv5, qdy, sy));
-        sz = fmaf(cc, dz, fmaf(-rinv5, qdz, sz));
-        if (POT) sp = fmaf(-0.5f * q, rinv5, fmaf(-a.w, rinv, sp));
+        sx = fmaf(cc, dx, fmaf(rinv5, qdx, sx));
+        sy = fmaf(cc, dy, fmaf(rinv5, qdy, sy));
+        sz = fmaf(cc, dz, fmaf(rinv5, qdz, sz));
+        if (POT) sp = fmaf(0.5f * q, rinv5, fmaf(-a.w, rinv, sp));
     } else {
         const float mr3 = a.w * rinv3;
         sx = fmaf(mr3, dx, sx);
@@ -171,11 +175,155 @@ __device__ __forceinline__ void eval_batch(const float4* stage, int count, float
     if (POT) kahan_add(T.pot, T.cp, sp);
 }
 
-// Stage up to 32 cells (one per lane) and evaluate them.
-template <bool QUAD, bool POT>
+// ---- packed evaluation: two list entries per FP32 instruction --------------
+// Blackwell's .f32x2 add/mul/fma do two FP32 operations per issued
+// instruction at the FMA pipe's full FLOP rate, and this walk is bound by
+// instruction issue, not by the FMA pipe.  Entries are staged in pairs,
+// interleaved field by field, so one LDS.128 delivers a field of both.
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 pk(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 upk(f2 v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+    f2 d;
+    asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+    f2 d;
+    asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+    f2 d;
+    asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+struct PairAcc {
+    f2 x, y, z;
+};
+
+// Two body-cell interactions.  e[0] = (x0 x1 y0 y1), e[1] = (z0 z1 m0 m1),
+// e[2..4] = -G (Qxx, Qyy | Qzz, Qxy | Qxz, Qyz) of both cells.
+template <bool QUAD>
+__device__ __forceinline__ void pc_pair(const float4* e, f2 tx, f2 ty, f2 tz, f2 eps2, f2 neg25, PairAcc& s) {
+    const float4 p0 = e[0], p1 = e[1];
+    const f2 dx = sub2(pk(p0.x, p0.y), tx), dy = sub2(pk(p0.z, p0.w), ty), dz = sub2(pk(p1.x, p1.y), tz);
+    const f2 m = pk(p1.z, p1.w);
+    const f2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, eps2)));
+    const float2 r2s = upk(r2);
+    const f2 rinv = pk(rsqrtf(r2s.x), rsqrtf(r2s.y));
+    const f2 rinv2 = mul2(rinv, rinv);
+    const f2 rinv3 = mul2(rinv2, rinv);
+    if (QUAD) {
+        const float4 a = e[2], b = e[3], c = e[4];
+        const f2 qxx = pk(a.x, a.y), qyy = pk(a.z, a.w), qzz = pk(b.x, b.y), qxy = pk(b.z, b.w);
+        const f2 qxz = pk(c.x, c.y), qyz = pk(c.z, c.w);
+        const f2 qdx = fma2(qxz, dz, fma2(qxy, dy, mul2(qxx, dx)));
+        const f2 qdy = fma2(qyz, dz, fma2(qyy, dy, mul2(qxy, dx)));
+        const f2 qdz = fma2(qzz, dz, fma2(qyz, dy, mul2(qxz, dx)));
+        const f2 q = fma2(dz, qdz, fma2(dy, qdy, mul2(dx, qdx)));
+        const f2 cc = mul2(rinv3, fma2(q, mul2(mul2(neg25, rinv2), rinv2), m));
+        const f2 rinv5 = mul2(rinv3, rinv2);
+        s.x = fma2(cc, dx, fma2(rinv5, qdx, s.x));
+        s.y = fma2(cc, dy, fma2(rinv5, qdy, s.y));
+        s.z = fma2(cc, dz, fma2(rinv5, qdz, s.z));
+    } else {
+        const f2 mr3 = mul2(m, rinv3);
+        s.x = fma2(mr3, dx, s.x);
+        s.y = fma2(mr3, dy, s.y);
+        s.z = fma2(mr3, dz, s.z);
+    }
+}
+
+// Two body-body interactions.  e[0] = (x0 x1 y0 y1), e[1] = (z0 z1 m0 m1).
+__device__ __forceinline__ void pp_pair(const float4* e, f2 tx, f2 ty, f2 tz, f2 eps2, PairAcc& s) {
+    const float4 p0 = e[0], p1 = e[1];
+    const f2 dx = sub2(pk(p0.x, p0.y), tx), dy = sub2(pk(p0.z, p0.w), ty), dz = sub2(pk(p1.x, p1.y), tz);
+    const f2 m = pk(p1.z, p1.w);
+    const f2 r2 = fma2(dz, dz, fma2(dy, dy, fma2(dx, dx, eps2)));
+    const float2 r2s = upk(r2);
+    const f2 rinv = pk(rsqrtf(r2s.x), rsqrtf(r2s.y));
+    const f2 mr3 = mul2(mul2(m, rinv), mul2(rinv, rinv));
+    s.x = fma2(mr3, dx, s.x);
+    s.y = fma2(mr3, dy, s.y);
+    s.z = fma2(mr3, dz, s.z);
+}
+
+template <int NPAIRS, int STRIDE, bool PC, bool QUAD>
+__device__ __forceinline__ void run_pairs_fixed(const float4* stage, int p0, f2 tx, f2 ty, f2 tz, f2 eps2, f2 neg25,
+                                                PairAcc& s) {
+    const float4* e = stage + STRIDE * p0;
+#pragma unroll kWalkUnroll
+    for (int p = 0; p < NPAIRS; ++p) {
+        if (PC) pc_pair<QUAD>(e + STRIDE * p, tx, ty, tz, eps2, neg25, s);
+        else pp_pair(e + STRIDE * p, tx, ty, tz, eps2, s);
+    }
+}
+
+// Packed counterpart of eval_batch: pairs [slice*npairs/nslices, ...).
+template <int STRIDE, bool PC, bool QUAD>
+__device__ __forceinline__ void eval_batch_packed(const float4* stage, int count, float eps2, bool active, int slice,
+                                                  int nslices, Target& T) {
+    if (!active) return;
+    const f2 tx = pk(T.tx, T.tx), ty = pk(T.ty, T.ty), tz = pk(T.tz, T.tz);
+    const f2 e2 = pk(eps2, eps2), neg25 = pk(-2.5f, -2.5f);
+    PairAcc s{0ull, 0ull, 0ull};
+    const int npairs = (count + 1) >> 1;
+    if (NB_WALK_FIXED && npairs == 16 && nslices == 1) {
+        run_pairs_fixed<16, STRIDE, PC, QUAD>(stage, 0, tx, ty, tz, e2, neg25, s);
+    } else {
+        const int chunk = (npairs + nslices - 1) / nslices;
+        const int p0 = slice * chunk;
+        const int p1 = min(npairs, p0 + chunk);
+        for (int p = p0; p < p1; ++p) {
+            if (PC) pc_pair<QUAD>(stage + STRIDE * p, tx, ty, tz, e2, neg25, s);
+            else pp_pair(stage + STRIDE * p, tx, ty, tz, e2, s);
+        }
+    }
+    const float2 sx = upk(s.x), sy = upk(s.y), sz = upk(s.z);
+    kahan_add(T.ax, T.cx, sx.x + sx.y);
+    kahan_add(T.ay, T.cy, sy.x + sy.y);
+    kahan_add(T.az, T.cz, sz.x + sz.y);
+}
+
+// Stage up to 32 cells (one per lane) and evaluate them.  PACK stages them in
+// pairs for the .f32x2 path (lanes past `count` stage zero-mass entries).
+template <bool QUAD, bool POT, bool PACK>
 __device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count, const Tree& t, double gcx,
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
+    if (PACK) {
+        float* f = reinterpret_cast<float*>(L.stage + 5 * (lane >> 1)) + (lane & 1);
+        float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (lane < count) {
+            const int node = list[lane];
+            const double4 c = t.com[node];
+            v[0] = static_cast<float>(c.x - gcx);
+            v[1] = static_cast<float>(c.y - gcy);
+            v[2] = static_cast<float>(c.z - gcz);
+            v[3] = static_cast<float>(G * c.w);
+            if (QUAD) {
+                const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
+                v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+        __syncwarp();
+        eval_batch_packed<5, true, QUAD>(L.stage, count, eps2, active, slice, nslices, T);
+        __syncwarp();
+        return;
+    }
     if (lane < count) {
         const int node = list[lane];
         const double4 c = t.com[node];
@@ -192,10 +340,27 @@ __device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count
 }
 
 // Stage up to 32 bodies (one per lane) and evaluate them.
-template <bool SOFT, bool POT>
+template <bool SOFT, bool POT, bool PACK>
 __device__ __forceinline__ void eval_pp(WarpLists& L, const int* list, int count, const Bodies& bd, double gcx,
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
+    if (PACK) {
+        float* f = reinterpret_cast<float*>(L.stage + 2 * (lane >> 1)) + (lane & 1);
+        float v[4] = {0, 0, 0, 0};
+        if (lane < count) {
+            const int j = list[lane];
+            v[0] = static_cast<float>(bd.x[j] - gcx);
+            v[1] = static_cast<float>(bd.y[j] - gcy);
+            v[2] = static_cast<float>(bd.z[j] - gcz);
+            v[3] = static_cast<float>(G * bd.m[j]);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+        __syncwarp();
+        eval_batch_packed<2, false, false>(L.stage, count, eps2, active, slice, nslices, T);
+        __syncwarp();
+        return;
+    }
     if (lane < count) {
         const int j = list[lane];
         L.stage[lane] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
@@ -211,6 +376,8 @@ __global__ void __launch_bounds__(128, NB_WALK_MIN_BLOCKS)
 walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int stack_cap, unsigned int* queue,
                   unsigned long long* stats, int* err, int64_t own_lo, int64_t own_hi) {
     if (*err & kErrAbort) return;
+    // softened forces without the potential take the packed two-entry path
+    constexpr bool kPack = NB_WALK_PACKED && SOFT && !POT;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
@@ -313,7 +480,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
             if (pc_n >= 32) {
-                eval_pc<QUAD, POT>(L, L.pc, 32, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
+                eval_pc<QUAD, POT, kPack>(L, L.pc, 32, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
                 g_pc += 32;
                 pc_n -= 32;
                 const int v = lane < pc_n ? L.pc[32 + lane] : 0;
@@ -334,7 +501,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
                 __syncwarp();
                 int head = 0;
                 while (pp_n - head >= 32) {
-                    eval_pp<SOFT, POT>(L, L.pp + head, 32, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
+                    eval_pp<SOFT, POT, kPack>(L, L.pp + head, 32, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
                     g_pp += 32;
                     head += 32;
                 }
@@ -351,8 +518,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrStack);
             continue;
         }
-        if (pc_n > 0) { eval_pc<QUAD, POT>(L, L.pc, pc_n, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
-        if (pp_n > 0) { eval_pp<SOFT, POT>(L, L.pp, pp_n, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
+        if (pc_n > 0) { eval_pc<QUAD, POT, kPack>(L, L.pc, pc_n, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
+        if (pp_n > 0) { eval_pp<SOFT, POT, kPack>(L, L.pp, pp_n, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
         double fx = static_cast<double>(T.ax) - static_cast<double>(T.cx);
         double fy = static_cast<double>(T.ay) - static_cast<double>(T.cy);
         double fz = static_cast<double>(T.az) - static_cast<double>(T.cz);
