@@ -1,13 +1,14 @@
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs: one histogram
 // pass over the keys for all digits, then one "onesweep" pass per 8-bit
 // digit.  Each onesweep pass ranks a tile of keys in shared memory (warp
-// match-any multisplit), publishes the tile's per-digit counts, and finds
+// ballot multisplit), publishes the tile's per-digit counts, and finds
 // the counts of all earlier tiles by decoupled look-back over a status
 // array (flag + count packed in one 32-bit word), so a pass reads and
-// writes every pair exactly once.  Tiles are numbered in the order blocks
-// start (an atomic ticket), so every tile a block waits on is already
-// running; each wait is still bounded and raises NEXT_DEVERR_SORT_TIMEOUT
-// instead of spinning forever.
+// writes every pair exactly once.  The look-back's first read is in flight
+// while the tile scans and scatters its keys locally.  Tiles are numbered
+// in the order blocks start (an atomic ticket), so every tile a block waits
+// on is already running; each wait is still bounded and raises
+// NEXT_DEVERR_SORT_TIMEOUT instead of spinning forever.
 //
 // Memory bound: per pass 12 B read + 12 B written per pair.
 #include "common.cuh"
@@ -61,11 +62,25 @@ __global__ void __launch_bounds__(kRadix) digit_offsets_kernel(const uint32_t* h
 struct SortSmem {
     uint32_t warp_hist[kWarps][kRadix];
     uint32_t tile_start[kRadix];
-    uint32_t global_base[kRadix];
+    uint32_t global_delta[kRadix];
+    uint32_t warp_total[kWarps];
     uint64_t keys[kTile];
     uint32_t vals[kTile];
     int tile;
 };
+
+// Lanes of the warp whose 8-bit digit equals this lane's: eight ballots,
+// one per digit bit (cheaper than a match-any on this part).
+__device__ __forceinline__ uint32_t digit_peers(int dig) {
+    uint32_t peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const bool bit = (dig >> b) & 1;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+    }
+    return peers;
+}
 
 __global__ void __launch_bounds__(kThreads)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
@@ -97,7 +112,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const uint32_t peers = __match_any_sync(0xffffffffu, dig[k]);
+        const uint32_t peers = digit_peers(dig[k]);
         const uint32_t before = S.warp_hist[w][dig[k]];
         rank[k] = before + __popc(peers & lt);
         __syncwarp();
@@ -105,7 +120,9 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         __syncwarp();
     }
     __syncthreads();
-    // Per digit: exclusive prefix over warps, tile count, look-back.
+    // Per digit d: exclusive prefix over warps and the tile count, published
+    // at once; the first look-back read is issued now and consumed after the
+    // local scan and scatter, which do not need it.
     const int d = threadIdx.x;
     uint32_t count = 0;
     for (int ww = 0; ww < kWarps; ++ww) {
@@ -116,33 +133,19 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     volatile uint32_t* vstat = status;
     if (tile == 0) vstat[d] = kFlagInc | count;
     else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
-    uint32_t excl = 0;
-    if (tile > 0) {
-        int pred = tile - 1;
-        while (pred >= 0) {
-            uint32_t v = vstat[static_cast<int64_t>(pred) * kRadix + d];
-            int spins = 0;
-            while ((v & (kFlagAgg | kFlagInc)) == 0) {
-                if (++spins > kSpinLimit) { raise_error(err, kErrSort); break; }
-                v = vstat[static_cast<int64_t>(pred) * kRadix + d];
-            }
-            excl += v & kCountMask;
-            if ((v & kFlagInc) || spins > kSpinLimit) break;
-            --pred;
-        }
-        vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
+    uint32_t v = tile > 0 ? vstat[static_cast<int64_t>(tile - 1) * kRadix + d] : 0u;
+    // Exclusive scan of the tile counts over digits: warp scans + warp totals.
+    uint32_t inc = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
     }
-    S.global_base[d] = digit_offsets[d] + excl;
-    // Exclusive scan of the tile counts over digits (local layout).
-    S.tile_start[d] = count;
+    if (lane == 31) S.warp_total[w] = inc;
     __syncthreads();
-    for (int o = 1; o < kRadix; o <<= 1) {
-        const uint32_t v = d >= o ? S.tile_start[d - o] : 0u;
-        __syncthreads();
-        S.tile_start[d] += v;
-        __syncthreads();
-    }
-    S.tile_start[d] -= count;
+    uint32_t tile_start = inc - count;
+    for (int ww = 0; ww < w; ++ww) tile_start += S.warp_total[ww];
+    S.tile_start[d] = tile_start;
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
@@ -150,12 +153,31 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         S.keys[pos] = key[k];
         S.vals[pos] = val[k];
     }
+    // Decoupled look-back for digit d over the earlier tiles.
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int pred = tile - 1;
+        for (;;) {
+            int spins = 0;
+            while ((v & (kFlagAgg | kFlagInc)) == 0) {
+                if (++spins > kSpinLimit) { raise_error(err, kErrSort); break; }
+                v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+            }
+            excl += v & kCountMask;
+            if ((v & kFlagInc) || spins > kSpinLimit || pred == 0) break;
+            --pred;
+            v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+        }
+        vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
+    }
+    // global position of local slot i with digit d: global_delta[d] + i
+    S.global_delta[d] = digit_offsets[d] + excl - tile_start;
     __syncthreads();
     const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
     for (int i = threadIdx.x; i < valid; i += kThreads) {
         const uint64_t k = S.keys[i];
         const int dd = static_cast<int>((k >> shift) & 0xff);
-        const uint32_t gpos = S.global_base[dd] + (static_cast<uint32_t>(i) - S.tile_start[dd]);
+        const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
         if (gpos >= n) { raise_error(err, kErrIndex); continue; }
         keys_out[gpos] = k;
         vals_out[gpos] = S.vals[i];

@@ -15,6 +15,9 @@
 // nodes are laid out sibling-contiguous (children of a node consecutive, in
 // octant order, system roots first) for the walks.
 //
+// Child bounds: one thread per internal cell runs the eight lower-bound
+// searches for the cell's end and child starts together.
+//
 // Upward pass: one thread per leaf computes the leaf's moments, then climbs;
 // at each parent an atomic arrival counter elects the last child's thread to
 // combine all children in octant order (deterministic), and that thread
@@ -49,22 +52,6 @@ __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf
     nint[s] = max(0, top - static_cast<int>(dlev[s]));
 }
 
-__device__ __forceinline__ int64_t lower_bound_key(const uint64_t* keys, int64_t lo, int64_t hi, uint64_t v) {
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (keys[mid] < v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ int64_t upper_bound_key(const uint64_t* keys, int64_t lo, int64_t hi, uint64_t v) {
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (keys[mid] <= v) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
 // Walk groups from the children of one cell holding more than G bodies:
 // consecutive children of at most G bodies are packed while the total stays
 // <= G; a child of more than G bodies that is a leaf (deepest level) is cut
@@ -93,45 +80,73 @@ __device__ int pack_groups(const int32_t* b, int level, int levels, int leaf_cap
     return ng;
 }
 
-__global__ void internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int8_t* __restrict__ dlev,
-                                const int32_t* __restrict__ int_base, const int32_t* __restrict__ sysid,
-                                const int64_t* __restrict__ offsets, int base, int levels, int leaf_cap,
-                                int group_cap, int64_t cap_int, Tree t, int* err) {
+// Internal cell ids: position s starts the cells q = int_base[s] + k at
+// levels dlev[s] + 1 + k.  Compacts them so the search kernel below runs one
+// thread per cell rather than per position.
+__global__ void cell_starts_kernel(const int8_t* __restrict__ dlev, const int32_t* __restrict__ int_base,
+                                   int64_t n, Tree t, int* err) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= n) return;
-    const int cnt = int_base[s + 1] - int_base[s];
+    const int q0 = int_base[s];
+    const int cnt = int_base[s + 1] - q0;
     if (cnt == 0) return;
     const int d = dlev[s];
-    const int sys = sysid ? sysid[s] : 0;
-    int64_t e_prev = offsets ? offsets[sys + 1] : n;
-    const uint64_t ks = keys[s];
     for (int k = 0; k < cnt; ++k) {
-        const int l = d + 1 + k;
-        const int64_t q = static_cast<int64_t>(int_base[s]) + k;
+        const int64_t q = static_cast<int64_t>(q0) + k;
         if (q >= t.cap_int) { raise_error(err, kErrTree); return; }
+        t.int_start[q] = static_cast<int32_t>(s);
+        t.int_level[q] = static_cast<int8_t>(d + 1 + k);
+    }
+}
+
+// Child boundaries of every internal cell (l, s): the cell ends at the first
+// key above its prefix, and child c starts at the first key >= prefix | c at
+// level l+1.  All eight are lower bounds over the same range [s, system end),
+// run together with one shared step sequence (the range halves every step
+// whatever the comparisons give), so a thread has eight independent loads in
+// flight per step and no divergence.
+__global__ void __launch_bounds__(256)
+internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int32_t* __restrict__ sysid,
+                const int64_t* __restrict__ offsets, int base, int levels, int leaf_cap, int group_cap, Tree t,
+                int* err) {
+    if (*err & kErrAbort) return;
+    const int64_t m = t.counts[0] < t.cap_int ? t.counts[0] : t.cap_int;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+        const int s = t.int_start[q];
+        const int l = t.int_level[q];
+        if (s < 0 || s >= n || l < 0 || l >= levels) { raise_error(err, kErrIndex); continue; }
+        const int64_t hi = offsets ? offsets[(sysid ? sysid[s] : 0) + 1] : n;
+        const uint64_t ks = keys[s];
         const int sh = base - 3 * l;                       // bits below level l's digits
         const uint64_t low = (sh >= 64) ? ~0ull : ((1ull << sh) - 1ull);
         const uint64_t prefix = ks & ~low;
-        const int64_t e = upper_bound_key(keys, s + 1, e_prev, prefix | low);
-        int32_t b[9];
-        b[0] = static_cast<int32_t>(s);
-        b[8] = static_cast<int32_t>(e);
-        const int csh = base - 3 * (l + 1);
-        int64_t lo = s;
-        for (int c = 1; c < 8; ++c) {
-            lo = lower_bound_key(keys, lo, e, prefix | (static_cast<uint64_t>(c) << csh));
-            b[c] = static_cast<int32_t>(lo);
+        const int csh = sh - 3;
+        uint64_t v[8];
+        v[0] = (prefix | low) + 1ull;                      // end of the cell
+#pragma unroll
+        for (int c = 1; c < 8; ++c) v[c] = prefix | (static_cast<uint64_t>(c) << csh);
+        int64_t pos[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) pos[c] = s;
+        int64_t len = hi - s;
+        while (len > 1) {
+            const int64_t half = len >> 1;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) pos[c] = __ldg(keys + pos[c] + half) < v[c] ? pos[c] + half : pos[c];
+            len -= half;
         }
+        int32_t b[9];
+        b[0] = s;
+#pragma unroll
+        for (int c = 1; c < 8; ++c) b[c] = static_cast<int32_t>(pos[c] + (__ldg(keys + pos[c]) < v[c] ? 1 : 0));
+        b[8] = static_cast<int32_t>(pos[0] + (__ldg(keys + pos[0]) < v[0] ? 1 : 0));
         int nchild = 0;
         for (int c = 0; c < 8; ++c) nchild += b[c + 1] > b[c];
         int ngroups = 0;
-        if (e - s > group_cap)
+        if (b[8] - b[0] > group_cap)
             ngroups = pack_groups(b, l, levels, leaf_cap, group_cap, [](int, int) {});
-        t.int_start[q] = static_cast<int32_t>(s);
-        t.int_level[q] = static_cast<int8_t>(l);
         for (int c = 0; c < 9; ++c) t.int_bounds[9 * q + c] = b[c];
         t.int_packed[q] = static_cast<int64_t>(nchild) | (static_cast<int64_t>(ngroups) << 32);
-        e_prev = e;
     }
 }
 
@@ -297,6 +312,12 @@ __device__ double rcrit_of(const Mom& a, uint64_t key, int level, double4 cube, 
     return 2.0 * half / theta + sqrt(ox * ox + oy * oy + oz * oz);
 }
 
+__device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
+    int old;
+    asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
+}
+
 __global__ void upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                               const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P,
                               Tree t, int* err) {
@@ -357,11 +378,10 @@ __global__ void upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __rest
                 raise_error(err, kErrIndex);
                 break;
             }
-            __threadfence();
-            const int old = atomicAdd(t.counter + q, 1);
+            // release this child's moments / acquire the siblings' ones
+            const int old = arrive_acq_rel(t.counter + q);
             if (old != plk.y - 1) break;
             t.counter[q] = 0;                      // re-armed for the next build
-            __threadfence();
             const int pl = t.int_level[q];
             const int ps = t.int_start[q];
             const double4 pcube = cubes[sysid ? sysid[ps] : 0];
@@ -419,9 +439,12 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
     cudaError_t e = exclusive_scan<int32_t>(t.nint, t.nint, n, nullptr, static_cast<int32_t*>(scan_tmp),
                                             t.counts + 0, st);
     if (e != cudaSuccess) return e;
-    if (n > 0)
-        internal_kernel<<<blocks, threads, 0, st>>>(keys, n, t.dlev, t.nint, sid, offs, sys.base, sys.levels,
-                                                    leaf_cap, group_cap, t.cap_int, t, err);
+    if (n > 0) {
+        cell_starts_kernel<<<blocks, threads, 0, st>>>(t.dlev, t.nint, n, t, err);
+        const unsigned iblocks = static_cast<unsigned>((t.cap_int + threads - 1) / threads);
+        internal_kernel<<<iblocks < 4096u ? (iblocks ? iblocks : 1u) : 4096u, threads, 0, st>>>(
+            keys, n, sid, offs, sys.base, sys.levels, leaf_cap, group_cap, t, err);
+    }
     e = exclusive_scan<int64_t>(t.int_packed, t.int_packed, t.cap_int, t.counts + 0,
                                 static_cast<int64_t*>(scan_tmp), nullptr, st);
     if (e != cudaSuccess) return e;
@@ -436,7 +459,7 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
     Params Pu = P;
     upward_kernel<<<ublocks < 8192u ? ublocks : 8192u, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu,
                                                                          t, err);
-    count_launches(n > 0 ? 8 : 5);
+    count_launches(n > 0 ? 9 : 5);
     return cudaGetLastError();
 }
 
