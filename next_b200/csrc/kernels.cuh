@@ -16,7 +16,10 @@ cudaError_t launch_keys(const Bodies& b, const int32_t* sysid, int64_t n, const 
                         uint32_t* idx, cudaStream_t st);
 
 // sort.cu
-constexpr int64_t kSortTile = 256 * 15;   // pairs per onesweep tile (threads x items)
+#ifndef NB_SORT_ITEMS
+#define NB_SORT_ITEMS 15
+#endif
+constexpr int64_t kSortTile = 256 * NB_SORT_ITEMS;   // pairs per onesweep tile (threads x items)
 constexpr int64_t sort_scratch_words_for(int64_t n) {
     return 2 * 8 * 256 + 8 + 8 * ((n + kSortTile - 1) / kSortTile) * 256;
 }

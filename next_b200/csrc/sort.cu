@@ -1,11 +1,15 @@
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs: one histogram
 // pass over the keys for all digits, then one "onesweep" pass per 8-bit
-// digit.  Each onesweep pass ranks a tile of keys in shared memory (warp
-// ballot multisplit), publishes the tile's per-digit counts, and finds
-// the counts of all earlier tiles by decoupled look-back over a status
-// array (flag + count packed in one 32-bit word), so a pass reads and
-// writes every pair exactly once.  The look-back's first read is in flight
-// while the tile scans and scatters its keys locally.  Tiles are numbered
+// digit.  A onesweep pass works on tiles of 256 x 15 pairs:
+//   1. load the tile, count its digits per warp (ballot peer masks, one
+//      shared add per digit group) and publish the per-digit tile counts
+//      in a status array (flag + count packed in one 32-bit word);
+//   2. read the statuses of the 8 preceding tiles (decoupled look-back),
+//      and while those loads are in flight scan the counts and rank and
+//      scatter the tile into shared memory in digit order;
+//   3. finish the look-back, publish the inclusive counts, and write the
+//      tile out, each digit run to its global offset,
+// so a pass reads and writes every pair exactly once.  Tiles are numbered
 // in the order blocks start (an atomic ticket), so every tile a block waits
 // on is already running; each wait is still bounded and raises
 // NEXT_DEVERR_SORT_TIMEOUT instead of spinning forever.
@@ -21,12 +25,13 @@ namespace {
 constexpr int kRadix = 256;
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 15;
-constexpr int kTile = kThreads * kItems;   // 3840 pairs
+constexpr int kItems = NB_SORT_ITEMS;
+constexpr int kTile = kThreads * kItems;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 20;
+constexpr int kLookWindow = 8;   // earlier tiles whose status one look-back step reads
 
 __global__ void __launch_bounds__(kThreads)
 histogram_kernel(const uint64_t* __restrict__ keys, int64_t n, int passes, uint32_t* __restrict__ hist) {
@@ -61,7 +66,6 @@ __global__ void __launch_bounds__(kRadix) digit_offsets_kernel(const uint32_t* h
 
 struct SortSmem {
     uint32_t warp_hist[kWarps][kRadix];
-    uint32_t tile_start[kRadix];
     uint32_t global_delta[kRadix];
     uint32_t warp_total[kWarps];
     uint64_t keys[kTile];
@@ -70,19 +74,32 @@ struct SortSmem {
 };
 
 // Lanes of the warp whose 8-bit digit equals this lane's: eight ballots,
-// one per digit bit (cheaper than a match-any on this part).
+// one per digit bit (cheaper than a match-any on this part).  Written as one
+// volatile block that is also ordered with memory accesses, so the compiler
+// neither hoists the bit tests of all items nor keeps them in registers.
 __device__ __forceinline__ uint32_t digit_peers(int dig) {
-    uint32_t peers = 0xffffffffu;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const bool bit = (dig >> b) & 1;
-        const uint32_t m = __ballot_sync(0xffffffffu, bit);
-        peers &= bit ? m : ~m;
-    }
+    uint32_t peers;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t.reg .u32 t, m, r;\n\t" "mov.u32 r, 0xffffffff;\n\t"
+        "and.b32 t, %1, 1;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 2;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 4;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 8;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 16;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 32;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 64;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "and.b32 t, %1, 128;\n\t" "setp.ne.u32 p, t, 0;\n\t" "vote.sync.ballot.b32 m, p, 0xffffffff;\n\t" "@!p not.b32 m, m;\n\t" "and.b32 r, r, m;\n\t"
+        "mov.u32 %0, r;\n\t}"
+        : "=r"(peers) : "r"(dig) : "memory");
     return peers;
 }
 
-__global__ void __launch_bounds__(kThreads)
+// Four resident blocks per SM (64 registers): the phases of one tile wait
+// on memory and on earlier tiles, so occupancy beats spill-free code here.
+#ifndef NB_SORT_MINB
+#define NB_SORT_MINB 4
+#endif
+__global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
                 const uint32_t* __restrict__ digit_offsets, uint32_t* status, unsigned int* tile_ticket,
@@ -97,32 +114,29 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     const int64_t tile_base = static_cast<int64_t>(tile) * kTile;
     const int64_t warp_base = tile_base + static_cast<int64_t>(w) * kItems * 32;
 
+    // Digits are re-extracted from the keys where needed: holding them (or
+    // anything derived from them) across the passes costs more registers.
     uint64_t key[kItems];
     uint32_t val[kItems];
-    int dig[kItems];
-    uint32_t rank[kItems];
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         const int64_t g = warp_base + k * 32 + lane;
-        if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; dig[k] = static_cast<int>((key[k] >> shift) & 0xff); }
-        else { key[k] = ~0ull; val[k] = 0u; dig[k] = kRadix - 1; }
+        if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; }
+        else { key[k] = ~0ull; val[k] = 0u; }
     }
-    // Warp-level multisplit in item order (stable: item k of every lane
-    // precedes item k+1, lanes in order within an item).
+    // Per-warp digit counts first (fire-and-forget shared adds by each digit's
+    // lowest lane), so the tile's counts are published before the ranking.
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const uint32_t peers = digit_peers(dig[k]);
-        const uint32_t before = S.warp_hist[w][dig[k]];
-        rank[k] = before + __popc(peers & lt);
-        __syncwarp();
-        if ((peers & lt) == 0) S.warp_hist[w][dig[k]] = before + __popc(peers);
-        __syncwarp();
+        const int dk = static_cast<int>((key[k] >> shift) & 0xff);
+        const uint32_t peers = digit_peers(dk);
+        if ((peers & lt) == 0) atomicAdd(&S.warp_hist[w][dk], static_cast<uint32_t>(__popc(peers)));
     }
     __syncthreads();
     // Per digit d: exclusive prefix over warps and the tile count, published
-    // at once; the first look-back read is issued now and consumed after the
-    // local scan and scatter, which do not need it.
+    // at once; the first look-back window is read now and consumed after the
+    // local scan and the ranking, which do not need it.
     const int d = threadIdx.x;
     uint32_t count = 0;
     for (int ww = 0; ww < kWarps; ++ww) {
@@ -133,7 +147,10 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     volatile uint32_t* vstat = status;
     if (tile == 0) vstat[d] = kFlagInc | count;
     else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
-    uint32_t v = tile > 0 ? vstat[static_cast<int64_t>(tile - 1) * kRadix + d] : 0u;
+    uint32_t win[kLookWindow];
+#pragma unroll
+    for (int j = 0; j < kLookWindow; ++j)
+        win[j] = tile - 1 - j >= 0 ? vstat[static_cast<int64_t>(tile - 1 - j) * kRadix + d] : static_cast<uint32_t>(kFlagInc);
     // Exclusive scan of the tile counts over digits: warp scans + warp totals.
     uint32_t inc = count;
 #pragma unroll
@@ -145,42 +162,68 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     __syncthreads();
     uint32_t tile_start = inc - count;
     for (int ww = 0; ww < w; ++ww) tile_start += S.warp_total[ww];
-    S.tile_start[d] = tile_start;
+    // warp_hist[w][d] becomes the first local slot of warp w's digit-d keys
+    for (int ww = 0; ww < kWarps; ++ww) S.warp_hist[ww][d] += tile_start;
     __syncthreads();
+    // Warp-level multisplit in item order (stable: item k of every lane
+    // precedes item k+1, lanes in order within an item), scattering each key
+    // to its local slot as it is ranked.
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const uint32_t pos = S.tile_start[dig[k]] + S.warp_hist[w][dig[k]] + rank[k];
+        const int dk = static_cast<int>((key[k] >> shift) & 0xff);
+        const uint32_t peers = digit_peers(dk);
+        const uint32_t base = S.warp_hist[w][dk];
+        const uint32_t pos = base + __popc(peers & lt);
+        __syncwarp();
+        if ((peers & lt) == 0) S.warp_hist[w][dk] = base + __popc(peers);
         S.keys[pos] = key[k];
         S.vals[pos] = val[k];
+        __syncwarp();
     }
-    // Decoupled look-back for digit d over the earlier tiles.
+    // Decoupled look-back for digit d over the earlier tiles, a window of
+    // statuses per step: entries are taken in order, an entry without a
+    // flag yet is re-read alone (bounded), the first inclusive one ends it.
     uint32_t excl = 0;
     if (tile > 0) {
         int pred = tile - 1;
-        for (;;) {
-            int spins = 0;
-            while ((v & (kFlagAgg | kFlagInc)) == 0) {
-                if (++spins > kSpinLimit) { raise_error(err, kErrSort); break; }
-                v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+        bool done = false, timed_out = false;
+        while (!done) {
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j) {
+                if (done) break;
+                uint32_t v = win[j];
+                int spins = 0;
+                while ((v & (kFlagAgg | kFlagInc)) == 0) {
+                    if (++spins > kSpinLimit) { timed_out = true; break; }
+                    v = vstat[static_cast<int64_t>(pred - j) * kRadix + d];
+                }
+                excl += v & kCountMask;
+                done = (v & kFlagInc) || timed_out || pred - j == 0;
             }
-            excl += v & kCountMask;
-            if ((v & kFlagInc) || spins > kSpinLimit || pred == 0) break;
-            --pred;
-            v = vstat[static_cast<int64_t>(pred) * kRadix + d];
+            if (done) break;
+            pred -= kLookWindow;
+#pragma unroll
+            for (int j = 0; j < kLookWindow; ++j)
+                win[j] = pred - j >= 0 ? vstat[static_cast<int64_t>(pred - j) * kRadix + d] : static_cast<uint32_t>(kFlagInc);
         }
+        if (timed_out) raise_error(err, kErrSort);
         vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
     }
     // global position of local slot i with digit d: global_delta[d] + i
     S.global_delta[d] = digit_offsets[d] + excl - tile_start;
     __syncthreads();
     const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
-    for (int i = threadIdx.x; i < valid; i += kThreads) {
-        const uint64_t k = S.keys[i];
-        const int dd = static_cast<int>((k >> shift) & 0xff);
-        const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
-        if (gpos >= n) { raise_error(err, kErrIndex); continue; }
-        keys_out[gpos] = k;
-        vals_out[gpos] = S.vals[i];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const int i = k * kThreads + threadIdx.x;
+        if (i < valid) {
+            const uint64_t kk = S.keys[i];
+            const int dd = static_cast<int>((kk >> shift) & 0xff);
+            const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
+            if (gpos >= n) { raise_error(err, kErrIndex); continue; }
+            keys_out[gpos] = kk;
+            vals_out[gpos] = S.vals[i];
+        }
     }
 }
 
