@@ -400,13 +400,12 @@ def run_ours(args):
         sim.sync()
         t0 = time.perf_counter()
         for _ in range(e_steps):
-            sim.upload_arrays(lanes)
-            sim.step(W["dt"])
-            sim.download({k: lanes[i] for i, k in enumerate(names)})
+            sim.step_host(lanes, W["dt"])
         te = time.perf_counter() - t0
         e2e = {"value": n * e_steps / te, "unit": "particle-steps/s", "h2d_bytes_per_step": 7 * 8 * n,
                "d2h_bytes_per_step": 6 * 8 * n, "steps": e_steps,
-               "path": "next_upload (pinned) + next_step + next_download (pinned) per step, host wall clock"}
+               "path": "next_step_host on pinned host arrays per step (the reference's Step(): upload, KDK step, "
+                       "positions copied back during the force phase, velocities after), host wall clock"}
         for p_ in ptrs:
             lib.next_host_free(p_)
     # ---- CPU baseline: the reference's own Step() on the host cores

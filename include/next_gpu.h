@@ -139,6 +139,15 @@ int next_step(next_handle* h, double dt);
  * captured CUDA graph. */
 int next_steps(next_handle* h, double dt, int nsteps);
 
+/* The reference's Step(ParticleSystem&, dt) on host arrays (src/gravity/
+ * step.h:25): upload x..vz, m and type (type may be NULL), one KDK step, and
+ * the new positions and velocities written back into x..vz in place.  The
+ * same as next_upload + next_step + next_download, but the positions are
+ * copied back while the force phase runs.  Returns after every copy into
+ * the caller's arrays has finished. */
+int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, double* z,
+                   double* vx, double* vy, double* vz, const double* m, const int* type);
+
 /* Forces at the current positions (the quantity bhAccel accumulates,
  * octree.h:133), in the caller's order.  pot may be NULL; it is filled only
  * in accurate mode. */

@@ -92,6 +92,8 @@ struct next_handle {
     uint32_t* sort_scratch = nullptr;
     size_t sort_words = 0;
     double* stage = nullptr;          // 7 x n staging lanes (upload) / up to 10 x n (download)
+    cudaStream_t st_out = nullptr;    // host copies that overlap the force phase (next_step_host)
+    cudaEvent_t ev_out = nullptr;
     int* stype = nullptr;
     const double** lanes_dev = nullptr;
 
@@ -674,6 +676,8 @@ void next_destroy(next_handle* h) {
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->h_counts) cudaFreeHost(h->h_counts);
     if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->ev_out) cudaEventDestroy(h->ev_out);
+    if (h->st_out) cudaStreamDestroy(h->st_out);
     if (h->st) cudaStreamDestroy(h->st);
     delete h;
 }
@@ -787,6 +791,76 @@ int next_step(next_handle* h, double dt) {
     rc = set_dt(h, dt);
     if (rc) return rc;
     return step_once(h, !h->timing);
+}
+
+// Gather lanes of the working state into caller order in the staging area
+// (slot first_slot on) and queue their device -> host copies on stream cs.
+static int export_lanes(next_handle* h, const double* const* src, double* const* dst, int cnt, int first_slot,
+                        cudaStream_t cs) {
+    NB_TRY(cudaMemcpyAsync(h->lanes_dev, src, sizeof(double*) * cnt, cudaMemcpyHostToDevice, h->st), "lanes");
+    double* out = h->stage + static_cast<int64_t>(first_slot) * h->n;
+    NB_TRY(launch_gather_out(h->lanes_dev, cnt, h->inv, h->n, out, h->st), "gather out");
+    if (cs != h->st) {
+        NB_TRY(cudaEventRecord(h->ev_out, h->st), "export event");
+        NB_TRY(cudaStreamWaitEvent(cs, h->ev_out, 0), "export wait");
+    }
+    for (int c = 0; c < cnt; ++c)
+        NB_TRY(cudaMemcpyAsync(dst[c], out + static_cast<int64_t>(c) * h->n, sizeof(double) * h->n,
+                               cudaMemcpyDeviceToHost, cs), "download");
+    return NEXT_OK;
+}
+
+int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, double* z, double* vx, double* vy,
+                   double* vz, const double* m, const int* type) {
+    if (!h) return NEXT_ERR_INVALID_ARGUMENT;
+    if (!std::isfinite(dt)) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "dt must be finite");
+    int rc = next_upload(h, n, x, y, z, vx, vy, vz, m, type);
+    if (rc) return rc;
+    rc = set_dt(h, dt);
+    if (rc) return rc;
+    if (!h->st_out) {
+        NB_TRY(cudaStreamCreateWithFlags(&h->st_out, cudaStreamNonBlocking), "export stream");
+        NB_TRY(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming), "export event");
+    }
+    if (!(h->prm.reuse_forces && h->forces_valid)) {
+        rc = forces_checked(h, false);
+        if (rc) return rc;
+    }
+    Bodies bd = h->cur_bodies();
+    NB_TRY(launch_kick_drift(bd, h->n, h->dts, h->err, h->st), "kick-drift");
+    // the positions are final: their copies out run beside the force phase
+    // (the gather into caller order precedes the re-sort in stream order)
+    const double* pos[3] = {bd.x, bd.y, bd.z};
+    double* pos_out[3] = {x, y, z};
+    rc = export_lanes(h, pos, pos_out, 3, 0, h->st_out);
+    if (rc == NEXT_OK) rc = forces(h, false, nullptr);
+    if (rc == NEXT_OK) {
+        bd = h->cur_bodies();
+        const cudaError_t e = launch_kick(bd, h->n, h->dts, h->err, h->st);
+        if (e != cudaSuccess) rc = cuda_fail(h, e, "kick");
+    }
+    const cudaError_t es = cudaStreamSynchronize(h->st_out);   // no copy into the caller's arrays outlives the call
+    if (rc) return rc;
+    if (es != cudaSuccess) return cuda_fail(h, es, "position copies");
+    int bits = 0;
+    rc = read_device_error(h, &bits);
+    if (rc) return rc;
+    if (bits) {
+        // the kick-drift ran and the positions are out; redo the force phase and the closing kick
+        rc = recover(h, bits);
+        if (rc) return rc;
+        rc = forces_checked(h, false);
+        if (rc) return rc;
+        bd = h->cur_bodies();
+        NB_TRY(launch_kick(bd, h->n, h->dts, h->err, h->st), "kick");
+    }
+    const double* vel[3] = {bd.vx, bd.vy, bd.vz};
+    double* vel_out[3] = {vx, vy, vz};
+    rc = export_lanes(h, vel, vel_out, 3, 3, h->st);
+    const cudaError_t ev = cudaStreamSynchronize(h->st);
+    if (rc) return rc;
+    if (ev != cudaSuccess) return cuda_fail(h, ev, "sync");
+    return NEXT_OK;
 }
 
 int next_steps(next_handle* h, double dt, int nsteps) {

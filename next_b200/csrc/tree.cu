@@ -318,7 +318,15 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
     return old;
 }
 
-__global__ void upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
+#ifndef NB_UP_MINB
+#define NB_UP_MINB 4
+#endif
+#if NB_UP_MINB > 0
+__global__ void __launch_bounds__(256, NB_UP_MINB)
+#else
+__global__ void
+#endif
+upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                               const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P,
                               Tree t, int* err) {
     if (*err & kErrAbort) return;

@@ -84,6 +84,23 @@ public:
 
     void step(double dt) { check(next_step(h_, dt), "step"); }
 
+    // Upload, one step and the copy back in one call; the positions travel
+    // back while the force phase runs.
+    void step_host(Particle& ps, double dt) {
+        const int64_t n = static_cast<int64_t>(ps.size());
+#if defined(NEXT_FP32)
+        std::vector<double> lanes[7];
+        std::vector<real>* src[7] = {&ps.x, &ps.y, &ps.z, &ps.vx, &ps.vy, &ps.vz, &ps.m};
+        for (int c = 0; c < 7; ++c) lanes[c].assign(src[c]->begin(), src[c]->end());
+        check(next_step_host(h_, dt, n, lanes[0].data(), lanes[1].data(), lanes[2].data(), lanes[3].data(),
+                             lanes[4].data(), lanes[5].data(), lanes[6].data(), ps.type.data()), "step");
+        for (int c = 0; c < 6; ++c) src[c]->assign(lanes[c].begin(), lanes[c].end());
+#else
+        check(next_step_host(h_, dt, n, ps.x.data(), ps.y.data(), ps.z.data(), ps.vx.data(), ps.vy.data(),
+                             ps.vz.data(), ps.m.data(), ps.type.data()), "step");
+#endif
+    }
+
     double adaptive_dt(double base) {
         double dt = base;
         check(next_adaptive_dt(h_, base, &dt), "adaptive dt");

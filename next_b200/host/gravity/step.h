@@ -3,7 +3,7 @@
 // kick dt/2 with forces at x_n, drift dt, kick dt/2 with forces at x_{n+1}.
 // The bodies are uploaded (forces cached from the previous call are kept when
 // the positions did not change), stepped on the device and copied back into
-// ps.  Unlike the reference, failures throw std::runtime_error, and bodies at
+// ps, the positions while the force phase still runs.  Unlike the reference, failures throw std::runtime_error, and bodies at
 // identical positions share a leaf instead of recursing without end.
 #pragma once
 #include "../floatdef.h"
@@ -12,8 +12,5 @@
 
 inline void Step(ParticleSystem& ps, real dt) {
     if (ps.size() == 0) return;   // as src/gravity/step.h:26
-    next_gpu::Engine& e = next_gpu::engine();
-    e.upload(ps);
-    e.step(static_cast<double>(dt));
-    e.download(ps);
+    next_gpu::engine().step_host(ps, static_cast<double>(dt));
 }

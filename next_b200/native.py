@@ -56,6 +56,7 @@ SIGNATURES = {
     "next_download": (C.c_int, [_h, _d, _d, _d, _d, _d, _d]),
     "next_step": (C.c_int, [_h, C.c_double]),
     "next_steps": (C.c_int, [_h, C.c_double, C.c_int]),
+    "next_step_host": (C.c_int, [_h, C.c_double, C.c_int64, _d, _d, _d, _d, _d, _d, _d, _i32]),
     "next_accel": (C.c_int, [_h, _d, _d, _d, _d]),
     "next_adaptive_dt": (C.c_int, [_h, C.c_double, _d]),
     "next_direct_accel": (C.c_int, [_h, C.c_int64, _i64, _d, _d, _d, _d]),
@@ -206,6 +207,17 @@ class Simulation:
 
     def steps(self, dt: float, nsteps: int):
         self._check(self.lib.next_steps(self.h, float(dt), int(nsteps)), "steps")
+
+    def step_host(self, lanes, dt: float, t=None):
+        """One step on caller-owned float64 arrays, in place (the reference's Step()):
+        lanes = [x, y, z, vx, vy, vz, m]; positions and velocities are overwritten."""
+        n = int(lanes[0].shape[0])
+        for a in lanes:
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape[0] != n:
+                raise ValueError("step_host needs seven contiguous float64 arrays of one length")
+        rc = self.lib.next_step_host(self.h, float(dt), n, *(_p(a, _d) for a in lanes), _p(t, _i32))
+        self._check(rc, "step_host")
+        self.n = n
 
     def accel(self, potential: bool = False):
         n = self.n

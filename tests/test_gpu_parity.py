@@ -14,7 +14,7 @@ import pytest
 
 from golden_cases import NAMES, load
 from next_b200 import ic
-from next_b200.native import Simulation
+from next_b200.native import NextError, Simulation
 
 pytestmark = pytest.mark.gpu
 
@@ -238,6 +238,45 @@ def test_graph_steps_equal_eager_steps():
         np.testing.assert_array_equal(sa[c], sg[c])
     a.close()
     g.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_step_host_equals_upload_step_download(precision):
+    """next_step_host (Step() on host arrays, positions copied back during the
+    force phase) gives the same state as next_upload + next_step + next_download."""
+    b = ic.plummer(30_000, seed=12)
+    s = Simulation("accurate", precision)
+    h = Simulation("accurate", precision)
+    names = ("x", "y", "z", "vx", "vy", "vz", "m")
+    lanes = [np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names]
+    ref = {k: np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names}
+    for _ in range(3):
+        s.upload_arrays([ref[k] for k in names])
+        s.step(1e-3)
+        s.download(ref)
+        h.step_host(lanes, 1e-3)
+        for i, k in enumerate(names[:6]):
+            np.testing.assert_array_equal(lanes[i], ref[k])
+    assert s.stats()["device_error"] == 0 and h.stats()["device_error"] == 0
+    s.close()
+    h.close()
+
+
+def test_step_host_rejects_bad_input():
+    b = ic.plummer(1_000, seed=13)
+    h = Simulation("accurate", "mixed")
+    names = ("x", "y", "z", "vx", "vy", "vz", "m")
+    lanes = [np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names]
+    keep = [a.copy() for a in lanes]
+    lanes[0][5] = np.nan
+    with pytest.raises(NextError):
+        h.step_host(lanes, 1e-3)
+    for a, k in zip(lanes[1:], keep[1:]):
+        np.testing.assert_array_equal(a, k)      # nothing written back on failure
+    lanes[0][5] = keep[0][5]
+    with pytest.raises(NextError):
+        h.step_host(lanes, float("inf"))
+    h.close()
 
 
 def test_reuse_forces_matches_recompute():
