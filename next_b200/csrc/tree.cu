@@ -53,9 +53,12 @@ __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf
 }
 
 // Walk groups from the children of one cell holding more than G bodies:
-// consecutive children of at most G bodies are packed while the total stays
-// <= G; a child of more than G bodies that is a leaf (deepest level) is cut
-// into chunks of G.  emit(start, count) is called per group; returns count.
+// the bodies of consecutive children of at most G bodies are cut into runs
+// of G in key order (a child that does not fit tops the current run up to G
+// and starts the next one with the rest of its bodies), so most groups fill
+// a warp; a child of more than G bodies that is a leaf (deepest level) is
+// cut into chunks of G.  emit(start, count) is called per group; returns
+// the count.
 template <typename F>
 __device__ int pack_groups(const int32_t* b, int level, int levels, int leaf_cap, int group_cap, F emit) {
     int ng = 0, run_start = -1, run_cnt = 0;
@@ -65,8 +68,13 @@ __device__ int pack_groups(const int32_t* b, int level, int levels, int leaf_cap
         if (cnt <= group_cap) {
             if (run_start >= 0 && run_cnt + cnt <= group_cap) {
                 run_cnt += cnt;
+            } else if (run_start >= 0) {
+                // top the run up to group_cap with the first bodies of this
+                // child and go on with the rest of it: full warps
+                const int take = group_cap - run_cnt;
+                emit(run_start, group_cap); ++ng;
+                run_start = b[c] + take; run_cnt = cnt - take;
             } else {
-                if (run_start >= 0) { emit(run_start, run_cnt); ++ng; }
                 run_start = b[c]; run_cnt = cnt;
             }
         } else {
