@@ -38,6 +38,7 @@ FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
 # capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
 WALK_DRAM_BYTES = 56.51e6
+SORT_BYTES_PER_BODY = 8 * 24 + 8
 
 
 def env_rank():
@@ -445,6 +446,14 @@ def run_ours(args):
         "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
         "interactions_per_body": (st["pp_interactions"] + st["pc_interactions"]) / max(1, st["walk_launches"]) / total_bodies,
         "pp_fraction": st["pp_interactions"] / max(1, st["pp_interactions"] + st["pc_interactions"]),
+        "pp_interactions_per_s": st["pp_interactions"] / (st["ms_walk"] * 1e-3),
+        "pc_interactions_per_s": st["pc_interactions"] / (st["ms_walk"] * 1e-3),
+        # the key sort's algorithmic traffic: 8 passes x (12 B read + 12 B written) + the
+        # 8-byte histogram read, per body, over the bench's own sort stage time
+        "sort_hbm": {"bytes_per_body": SORT_BYTES_PER_BODY,
+                     "gbs": SORT_BYTES_PER_BODY * total_bodies / (st["ms_sort"] / args.steps * 1e-3) / 1e9,
+                     "frac": SORT_BYTES_PER_BODY * total_bodies / (st["ms_sort"] / args.steps * 1e-3) / 1e9 / peaks["hbm_gbs"]
+                     if peaks.get("hbm_gbs") else None},
         "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - st["n_systems"],
                  "bodies_per_group": n / max(1, st["n_groups"] - st["n_systems"]), "max_walk_stack": st["max_stack"]},
         "stage_ms_per_step": {"build": st["ms_build"] / args.steps, "sort": st["ms_sort"] / args.steps,

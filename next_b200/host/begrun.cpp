@@ -6,7 +6,9 @@
 // Each loop iteration takes dt = computeAdaptiveDt(bodies, dt_arg), runs one
 // KDK step, advances the simulation time and writes dump_<k>.<fmt> whenever
 // the time passes the next dump time; typing `q` (or `Q`) ends the run.  The
-// bodies stay on the GPU between steps and are copied back only for dumps.
+// bodies stay on the GPU between steps and are copied back only for dumps;
+// a dump's file is written by a host thread while the GPU runs the next
+// steps (the writer of one dump is waited for before the next copy back).
 //
 // Additions, all optional and off by default so the contract is unchanged:
 //   NEXT_MAX_STEPS / NEXT_T_END  stop after that many steps / that time
@@ -19,6 +21,7 @@
 #include <unistd.h>
 
 #include <cstdlib>
+#include <future>
 #include <iostream>
 #include <string>
 
@@ -88,16 +91,22 @@ int main(int argc, char** argv) {
         eng.upload(particles);
         double sim_time = 0, next_dump = 0;
         long dumps = 0, steps = 0;
+        std::future<void> writer;   // the previous dump's file, being written
         for (;;) {
             const double dt = eng.adaptive_dt(dt_arg);
             eng.step(dt);
             sim_time += dt;
             ++steps;
             if (sim_time >= next_dump) {
+                if (writer.valid()) writer.get();   // `particles` is free again
                 eng.download(particles);
-                std::string out = "dump_" + std::to_string(dumps);
-                if (format == Format::VTK) { out += ".vtk"; SaveVTK(particles, out); }
-                else { out += ".vtu"; SaveVTU(particles, out); }
+                std::string out = "dump_" + std::to_string(dumps) + (format == Format::VTK ? ".vtk" : ".vtu");
+                // only dumps touch `particles` (the state lives on the GPU), so the
+                // file can be written while the next steps run
+                writer = std::async(std::launch::async, [&particles, out, format] {
+                    if (format == Format::VTK) SaveVTK(particles, out);
+                    else SaveVTU(particles, out);
+                });
                 std::cout << "[Dump " << dumps << "] t = " << sim_time << ", file: " << out << std::endl;
                 next_dump += dump_interval;
                 ++dumps;
@@ -108,6 +117,7 @@ int main(int argc, char** argv) {
             }
             if ((max_steps >= 0 && steps >= max_steps) || (t_end >= 0 && sim_time >= t_end)) break;
         }
+        if (writer.valid()) writer.get();
     } catch (const std::exception& e) {
         std::cerr << "next: " << e.what() << std::endl;
         return 2;
