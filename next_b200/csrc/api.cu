@@ -189,7 +189,7 @@ int cuda_fail(next_handle* h, cudaError_t e, const char* where) {
 void free_tree(next_handle* h) {
     Tree& t = h->t;
     dfree(t.dlev); dfree(t.nint); dfree(t.int_start); dfree(t.int_level); dfree(t.int_bounds);
-    dfree(t.int_packed); dfree(t.int_node); dfree(t.counter); dfree(t.link); dfree(t.parent); dfree(t.level);
+    dfree(t.int_packed); dfree(t.int_node); dfree(t.counter); dfree(t.climb); dfree(t.link); dfree(t.parent); dfree(t.level);
     dfree(t.com); dfree(t.quad64); dfree(t.box); dfree(t.quad32); dfree(t.groups);
     dfree(h->scan_tmp);
     t.cap_int = t.cap_node = t.cap_group = 0;
@@ -215,7 +215,7 @@ int alloc_tree(next_handle* h, int64_t cap_int) {
     auto A = [&](auto** p, size_t c) { if (e == cudaSuccess) e = dalloc(p, c); };
     A(&t.dlev, n + 1); A(&t.nint, n + 1);
     A(&t.int_start, cap_int); A(&t.int_level, cap_int); A(&t.int_bounds, 9 * cap_int);
-    A(&t.int_packed, cap_int + 1); A(&t.int_node, cap_int); A(&t.counter, cap_int);
+    A(&t.int_packed, cap_int + 1); A(&t.int_node, cap_int); A(&t.counter, cap_int); A(&t.climb, cap_int);
     A(&t.link, t.cap_node); A(&t.parent, t.cap_node); A(&t.level, t.cap_node);
     A(&t.com, t.cap_node); A(&t.quad64, 8 * t.cap_node);
     if (h->P.physics == NEXT_PHYSICS_ACCURATE) { A(&t.box, t.cap_node); A(&t.quad32, 2 * t.cap_node); }

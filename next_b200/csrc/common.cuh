@@ -53,6 +53,7 @@ struct Tree {
     int64_t* int_packed;   // nchild | ngroups << 32 -> exclusive scan in place
     int32_t* int_node;     // node id of q
     int32_t* counter;      // upward-pass arrivals (self-resetting)
+    int4* climb;           // node id, first child, child count | level << 8, start position
     // per node
     int2* link;            // internal: (first child, nchild); leaf: (first body, -count)
     int32_t* parent;       // internal id of the parent (-1 for a root)

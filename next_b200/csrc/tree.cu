@@ -202,6 +202,7 @@ __global__ void children_kernel(const uint64_t* __restrict__ keys, const int8_t*
         if (l == 0) {
             t.int_node[q] = sys;
             t.link[sys] = make_int2(fc, nc);
+            t.climb[q] = make_int4(sys, fc, nc, s);
             t.parent[sys] = -1;
             t.level[sys] = 0;
         }
@@ -218,8 +219,10 @@ __global__ void children_kernel(const uint64_t* __restrict__ keys, const int8_t*
                 if (q2 <= q || q2 >= m) { raise_error(err, kErrIndex); return; }
                 t.int_node[q2] = nid;
                 const int64_t p2 = t.int_packed[q2], n2 = t.int_packed[q2 + 1];
-                t.link[nid] = make_int2(nsys + static_cast<int>(p2 & 0xffffffffll),
-                                        static_cast<int>((n2 & 0xffffffffll) - (p2 & 0xffffffffll)));
+                const int fc2 = nsys + static_cast<int>(p2 & 0xffffffffll);
+                const int nc2 = static_cast<int>((n2 & 0xffffffffll) - (p2 & 0xffffffffll));
+                t.link[nid] = make_int2(fc2, nc2);
+                t.climb[q2] = make_int4(nid, fc2, nc2 | ((l + 1) << 8), cs);
             } else {
                 t.link[nid] = make_int2(cs, -cnt);
             }
@@ -387,19 +390,22 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
         int q = t.parent[n];
         while (q >= 0) {
             if (q >= ninternal) { raise_error(err, kErrIndex); break; }
-            const int nid = t.int_node[q];
-            if (nid < 0 || nid >= nodes) { raise_error(err, kErrIndex); break; }
-            const int2 plk = t.link[nid];
-            if (plk.y < 1 || plk.y > 8 || plk.x < 0 || static_cast<int64_t>(plk.x) + plk.y > nodes) {
+            // the parent's record (written by the child-search pass) and the
+            // arrival both need only q: their round trips overlap
+            const int4 rec = __ldg(t.climb + q);
+            // release this child's moments / acquire the siblings' ones
+            const int old = arrive_acq_rel(t.counter + q);
+            const int nid = rec.x;
+            const int2 plk = make_int2(rec.y, rec.z & 0xff);
+            if (nid < 0 || nid >= nodes || plk.y < 1 || plk.y > 8 || plk.x < 0 ||
+                static_cast<int64_t>(plk.x) + plk.y > nodes) {
                 raise_error(err, kErrIndex);
                 break;
             }
-            // release this child's moments / acquire the siblings' ones
-            const int old = arrive_acq_rel(t.counter + q);
             if (old != plk.y - 1) break;
             t.counter[q] = 0;                      // re-armed for the next build
-            const int pl = t.int_level[q];
-            const int ps = t.int_start[q];
+            const int pl = rec.z >> 8;
+            const int ps = rec.w;
             const double4 pcube = cubes[sysid ? sysid[ps] : 0];
             const double phalf = ldexp(pcube.w, -pl);
             Mom p{};
