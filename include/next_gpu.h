@@ -98,6 +98,8 @@ typedef struct next_stats {
     double ms_sort;          /* ... of which radix sort */
     double ms_other;         /* ... kick/drift and the rest */
     int64_t walk_launches;   /* walks timed */
+    int32_t key_levels;      /* octant levels in the keys of the last build (21 = full depth) */
+    int32_t reserved;
 } next_stats;
 
 typedef struct next_handle next_handle;

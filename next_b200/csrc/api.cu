@@ -136,6 +136,12 @@ struct next_handle {
     // state
     bool have_bodies = false;
     bool forces_valid = false;
+    // octant levels held in the keys: the full 21 by default; the FP32-mixed
+    // walk of accurate physics trims them to the measured tree depth + 3 once
+    // per uploaded state (fewer FP64 key levels, fewer sort passes)
+    int sys_bits = 0;                 // bits of the system number above the octant digits
+    int key_bits = 63;                // sorted key bits
+    bool depth_decided = false;
     bool pot_valid = false;
     bool sorted_in_alt = false;
 
@@ -313,7 +319,8 @@ int build(next_handle* h, std::vector<int>* evs) {
     rc0 = record(h, evs);
     if (rc0) return rc0;
     bool in_alt = false;
-    NB_TRY(radix_sort_pairs(h->keys, h->idx, h->keys_alt, h->idx_alt, n, 63, h->sort_scratch, h->err, &in_alt, h->st),
+    NB_TRY(radix_sort_pairs(h->keys, h->idx, h->keys_alt, h->idx_alt, n, h->key_bits, h->sort_scratch, h->err, &in_alt,
+                            h->st),
            "radix sort");
     h->sorted_in_alt = in_alt;
     int rc = record(h, evs);
@@ -367,12 +374,38 @@ int forces(next_handle* h, bool potential, std::vector<int>* evs) {
     return record(h, evs);
 }
 
+// Octant levels of the keys (and the key layout that goes with them): the
+// full depth keeps the upload layout (system number from bit 63 - sys_bits
+// down), a trimmed depth packs the digits at the bottom.
+void set_key_levels(next_handle* h, int levels) {
+    Systems& S = h->sys;
+    const int full = std::min(kMaxLevel, (63 - h->sys_bits) / 3);
+    levels = std::max(1, std::min(levels, full));
+    const int base = levels == full ? 63 - h->sys_bits : 3 * levels;
+    if (S.levels != levels || S.base != base) drop_graphs(h);
+    S.levels = levels;
+    S.base = base;
+    h->key_bits = base + h->sys_bits;
+}
+
+bool adaptive_depth(const next_handle* h) {
+    return h->prm.precision == NEXT_PRECISION_MIXED && h->P.physics == NEXT_PHYSICS_ACCURATE;
+}
+
 int read_device_error(next_handle* h, int* bits) {
     NB_TRY(cudaMemcpyAsync(h->h_err, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->st), "error word");
-    NB_TRY(cudaMemcpyAsync(h->h_counts, h->t.counts, sizeof(int64_t) * 3, cudaMemcpyDeviceToHost, h->st), "counts");
+    NB_TRY(cudaMemcpyAsync(h->h_counts, h->t.counts, sizeof(int64_t) * 4, cudaMemcpyDeviceToHost, h->st), "counts");
     NB_TRY(cudaMemcpyAsync(h->h_stats, h->stats, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, h->st), "stats");
     NB_TRY(cudaStreamSynchronize(h->st), "sync");
     *bits = *h->h_err;
+    // the first build after an upload measured the tree depth: later builds
+    // keep three levels of margin below it (a deeper tree would only get
+    // leaves of more than leaf_cap bodies at the last level, still exact)
+    if (!h->depth_decided && *bits == 0 && h->h_counts[3] > 0) {
+        h->depth_decided = true;
+        if (adaptive_depth(h) && h->h_counts[3] + 3 < h->sys.levels)
+            set_key_levels(h, static_cast<int>(h->h_counts[3]) + 3);
+    }
     return NEXT_OK;
 }
 
@@ -709,15 +742,12 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
         h->n = n;
         Systems& S = h->sys;
         S.n = h->nsys;
-        if (h->nsys == 1) {
-            S.base = 63;
-            S.levels = kMaxLevel;
-        } else {
-            int bits = 0;
-            while ((int64_t(1) << bits) < n_systems) ++bits;
-            S.base = 63 - bits;
-            S.levels = std::min(kMaxLevel, S.base / 3);
-        }
+        int bits = 0;
+        while (h->nsys > 1 && (int64_t(1) << bits) < n_systems) ++bits;
+        h->sys_bits = bits;
+        S.levels = 0;
+        set_key_levels(h, kMaxLevel);
+        h->depth_decided = false;
         S.offsets = h->d_offsets;
         S.cube = h->cubes;
         set_share(h);
@@ -754,6 +784,8 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
     NB_TRY(launch_load_all(h->stage, h->stype, b, h->inv, n, h->st), "load");
     h->forces_valid = false;
     h->have_bodies = true;
+    set_key_levels(h, kMaxLevel);     // new positions: measure the depth again
+    h->depth_decided = false;
     return NEXT_OK;
 }
 
@@ -1022,6 +1054,7 @@ int next_stats_get(next_handle* h, next_stats* s) {
         s->n_internal = h->h_counts[0];
         s->n_nodes = h->h_counts[1];
         s->n_groups = h->h_counts[2];
+        s->key_levels = h->sys.levels;
         s->pp_interactions = static_cast<int64_t>(h->h_stats[0]);
         s->pc_interactions = static_cast<int64_t>(h->h_stats[1]);
         s->max_stack = static_cast<int64_t>(h->h_stats[2]);

@@ -39,17 +39,25 @@ __global__ void dlev_kernel(const uint64_t* __restrict__ keys, int64_t n, int ba
     dlev[s] = static_cast<int8_t>(s == 0 ? -1 : shared_levels(keys[s - 1], keys[s], base, levels));
 }
 
+// Internal cells starting at each position; *deepest gets the deepest leaf
+// level (one below the deepest internal cell) of the build.
 __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf_cap, int levels,
-                            int32_t* __restrict__ nint) {
+                            int32_t* __restrict__ nint, unsigned long long* deepest) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    int mb = -1;
-    if (s + leaf_cap < n) {
-        mb = 127;
-        for (int j = 1; j <= leaf_cap; ++j) mb = min(mb, static_cast<int>(dlev[s + j]));
+    unsigned deep = 0;
+    if (s < n) {
+        int mb = -1;
+        if (s + leaf_cap < n) {
+            mb = 127;
+            for (int j = 1; j <= leaf_cap; ++j) mb = min(mb, static_cast<int>(dlev[s + j]));
+        }
+        const int top = min(mb, levels - 1);
+        const int c = max(0, top - static_cast<int>(dlev[s]));
+        nint[s] = c;
+        if (c > 0) deep = static_cast<unsigned>(top + 1);
     }
-    const int top = min(mb, levels - 1);
-    nint[s] = max(0, top - static_cast<int>(dlev[s]));
+    deep = __reduce_max_sync(0xffffffffu, deep);
+    if ((threadIdx.x & 31) == 0 && deep) atomicMax(deepest, static_cast<unsigned long long>(deep));
 }
 
 // Walk groups from the children of one cell holding more than G bodies:
@@ -454,9 +462,12 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
     const int group_cap = P.group_cap < leaf_cap ? leaf_cap : P.group_cap;
     const int32_t* sid = sys.n > 1 ? sysid : nullptr;
     const int64_t* offs = sys.n > 1 ? d_offsets : nullptr;
+    cudaError_t e0 = cudaMemsetAsync(t.counts + 3, 0, sizeof(int64_t), st);
+    if (e0 != cudaSuccess) return e0;
     if (n > 0) {
         dlev_kernel<<<blocks, threads, 0, st>>>(keys, n, sys.base, sys.levels, t.dlev);
-        nint_kernel<<<blocks, threads, 0, st>>>(t.dlev, n, leaf_cap, sys.levels, t.nint);
+        nint_kernel<<<blocks, threads, 0, st>>>(t.dlev, n, leaf_cap, sys.levels, t.nint,
+                                                reinterpret_cast<unsigned long long*>(t.counts + 3));
     }
     cudaError_t e = exclusive_scan<int32_t>(t.nint, t.nint, n, nullptr, static_cast<int32_t*>(scan_tmp),
                                             t.counts + 0, st);

@@ -35,7 +35,8 @@ class Stats(C.Structure):
                 ("n_internal", C.c_int64), ("n_groups", C.c_int64), ("pp_interactions", C.c_int64),
                 ("pc_interactions", C.c_int64), ("max_stack", C.c_int64), ("device_error", C.c_int32),
                 ("steps", C.c_int32), ("ms_step", C.c_double), ("ms_build", C.c_double), ("ms_walk", C.c_double),
-                ("ms_sort", C.c_double), ("ms_other", C.c_double), ("walk_launches", C.c_int64)]
+                ("ms_sort", C.c_double), ("ms_other", C.c_double), ("walk_launches", C.c_int64),
+                ("key_levels", C.c_int32), ("reserved", C.c_int32)]
 
 
 # name -> (restype, argtypes)

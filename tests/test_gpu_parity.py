@@ -179,6 +179,35 @@ def test_mixed_precision_force_error(oracle, maker, n, theta, eps):
     sim.close()
 
 
+def test_mixed_steps_trim_key_depth(oracle):
+    """After the first build the FP32-mixed path keeps only the measured tree
+    depth + 3 octant levels in its keys; forces stay as accurate and match a
+    full-depth build of the same state (same tree, bodies within a leaf may be
+    in another order)."""
+    b = ic.plummer(60_000, seed=21)
+    sim = Simulation("accurate", "mixed", theta=0.5, eps=0.01)
+    sim.upload(b)
+    assert sim.stats()["key_levels"] == 21
+    sim.steps(1e-3, 3)
+    levels = sim.stats()["key_levels"]
+    assert 3 < levels < 21
+    a = sim.accel()
+    state = sim.download()
+    now = dict(b)
+    now.update(state)
+    full = Simulation("accurate", "mixed", theta=0.5, eps=0.01)
+    full.upload(now)
+    f = full.accel()
+    assert full.stats()["key_levels"] == 21 or full.stats()["key_levels"] == levels
+    assert np.median(rel_err(a, f)) <= 1e-5
+    idx = np.random.default_rng(1).choice(60_000, 1024, replace=False)
+    d = oracle.direct(now, idx, eps=0.01)
+    assert np.median(rel_err({c: a[c][idx] for c in a}, d)) <= 1e-3
+    assert sim.stats()["device_error"] == 0
+    sim.close()
+    full.close()
+
+
 def test_mixed_close_to_plain_accurate():
     b = ic.plummer(32_768, seed=6)
     plain = Simulation("accurate", "fp64", theta=0.5, eps=0.01, leaf_cap=16)
