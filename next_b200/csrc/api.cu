@@ -142,6 +142,8 @@ struct next_handle {
     int sys_bits = 0;                 // bits of the system number above the octant digits
     int key_bits = 63;                // sorted key bits
     bool depth_decided = false;
+    int64_t builds = 0;               // tree builds enqueued
+    int64_t depth_seen = 0;           // the build whose depth report was last acted on
     bool pot_valid = false;
     bool sorted_in_alt = false;
 
@@ -314,6 +316,7 @@ int build(next_handle* h, std::vector<int>* evs) {
     Bodies src = h->cur_bodies();
     int rc0 = record(h, evs);
     if (rc0) return rc0;
+    ++h->builds;
     NB_TRY(launch_root_cubes(src, n, h->sys, h->d_offsets, h->partial, kReduceMax, h->tickets + 0, h->st), "root cube");
     NB_TRY(launch_keys(src, h->sysid, n, h->sys, h->keys, h->idx, h->st), "keys");
     rc0 = record(h, evs);
@@ -399,13 +402,20 @@ int read_device_error(next_handle* h, int* bits) {
     NB_TRY(cudaStreamSynchronize(h->st), "sync");
     *bits = *h->h_err;
     // the first build after an upload measured the tree depth: later builds
-    // keep three levels of margin below it (a deeper tree would only get
-    // leaves of more than leaf_cap bodies at the last level, still exact)
-    if (!h->depth_decided && *bits == 0 && h->h_counts[3] > 0) {
-        h->depth_decided = true;
-        if (adaptive_depth(h) && h->h_counts[3] + 3 < h->sys.levels)
-            set_key_levels(h, static_cast<int>(h->h_counts[3]) + 3);
+    // keep three levels of margin below it.  A tree that outgrows them gets
+    // leaves of more than leaf_cap bodies at the last level (still exact,
+    // slower): seen here, the keys get three more levels.
+    const int64_t deepest = h->h_counts[3];
+    if (h->depth_seen == h->builds) return NEXT_OK;   // no build since the last look
+    h->depth_seen = h->builds;
+    if (*bits == 0 && deepest > 0 && adaptive_depth(h)) {
+        if (!h->depth_decided) {
+            if (deepest + 3 < h->sys.levels) set_key_levels(h, static_cast<int>(deepest) + 3);
+        } else if (deepest >= kDepthOverfull) {
+            set_key_levels(h, h->sys.levels + 3);
+        }
     }
+    if (*bits == 0 && deepest > 0) h->depth_decided = true;
     return NEXT_OK;
 }
 
@@ -494,6 +504,7 @@ int capture_step(next_handle* h) {
     const int saved_cur = h->cur;
     cudaGraph_t g = nullptr;
     const int64_t launches_before = launches_so_far();
+    const int64_t builds_before = h->builds;   // capturing runs nothing
     NB_TRY(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeRelaxed), "begin capture");
     int rc = NEXT_OK;
     Bodies bd = h->cur_bodies();
@@ -509,6 +520,7 @@ int capture_step(next_handle* h) {
         bd = h->cur_bodies();
         e = launch_kick(bd, h->n, h->dts, h->err, h->st);
     }
+    h->builds = builds_before;
     cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
     const int64_t captured = launches_so_far() - launches_before;
     count_launches(static_cast<int>(-captured));   // captured, not launched
@@ -930,6 +942,7 @@ int next_steps(next_handle* h, double dt, int nsteps) {
             if (rc) return rc;
         }
         NB_TRY(cudaGraphLaunch(h->graph[parity], h->st), "graph launch");
+        ++h->builds;                       // the replay's build
         count_launches(static_cast<int>(h->graph_kernels[parity]));
         if (h->timing) {
             // stage times of this replay: its in-graph events are overwritten by the next one

@@ -40,6 +40,10 @@ struct Systems {
 // the children of every internal node are stored consecutively in octant
 // order.  Internal nodes also have a depth-first "internal id" q used by the
 // build.
+// nint_kernel's depth report when leaf_cap + 1 bodies share a cell at the
+// last key level (a leaf over capacity: the keys need more levels)
+constexpr unsigned kDepthOverfull = 64;
+
 struct Tree {
     // capacities
     int64_t cap_int, cap_node, cap_group;

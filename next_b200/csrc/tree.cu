@@ -40,7 +40,8 @@ __global__ void dlev_kernel(const uint64_t* __restrict__ keys, int64_t n, int ba
 }
 
 // Internal cells starting at each position; *deepest gets the deepest leaf
-// level (one below the deepest internal cell) of the build.
+// level (one below the deepest internal cell) of the build, or
+// kDepthOverfull if a cell at the last key level holds more than leaf_cap.
 __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf_cap, int levels,
                             int32_t* __restrict__ nint, unsigned long long* deepest) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -55,6 +56,7 @@ __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf
         const int c = max(0, top - static_cast<int>(dlev[s]));
         nint[s] = c;
         if (c > 0) deep = static_cast<unsigned>(top + 1);
+        if (mb >= levels) deep = kDepthOverfull;
     }
     deep = __reduce_max_sync(0xffffffffu, deep);
     if ((threadIdx.x & 31) == 0 && deep) atomicMax(deepest, static_cast<unsigned long long>(deep));

@@ -208,6 +208,53 @@ def test_mixed_steps_trim_key_depth(oracle):
     full.close()
 
 
+def test_key_depth_grows_with_the_tree():
+    """Half the bodies fly ballistically (G = 0) into a small clump, so the
+    tree deepens past the trimmed key depth.  The leaf over capacity this
+    causes at the last key level is noticed at the next synchronisation and
+    the keys get more levels; once they suffice, the tree matches a
+    full-depth build of the same state."""
+    n = 24_576
+    b = ic.uniform_sphere(n, seed=7)
+    target = {"x": 0.3, "y": 0.2, "z": 0.1}
+    for ax in ("x", "y", "z"):
+        v = np.zeros(n)
+        v[n // 2:] = (target[ax] - b[ax][n // 2:]) / 0.95
+        b["v" + ax] = v
+    sim = Simulation("accurate", "mixed", theta=0.5, eps=0.001, G=0.0)
+    sim.upload(b)
+    sim.accel()
+    start = sim.stats()["key_levels"]
+    assert start < 21
+    sim.steps(0.3, 3)
+    for _ in range(8):
+        before = sim.stats()["key_levels"]
+        sim.reset_timers()
+        sim.steps(0.0, 1)            # a step of zero length: a new build at the same positions
+        if sim.stats()["key_levels"] == before:
+            break
+    st = sim.stats()
+    assert st["key_levels"] > start
+    now = dict(b)
+    now.update(sim.download())
+    full = Simulation("accurate", "mixed", theta=0.5, eps=0.001, G=0.0)
+    full.upload(now)
+    full.accel()
+    full.reset_timers()
+    full.steps(0.0, 1)
+    fs = full.stats()
+    keys = ("n_nodes", "n_internal", "n_groups")
+    assert tuple(st[k] for k in keys) == tuple(fs[k] for k in keys)
+    # groups may split a child at another body when bodies deeper than the
+    # key levels keep their previous order: totals agree to a fraction
+    mine = st["pp_interactions"] + st["pc_interactions"]
+    ref = fs["pp_interactions"] + fs["pc_interactions"]
+    assert abs(mine - ref) <= 0.01 * ref
+    assert st["device_error"] == 0 and fs["device_error"] == 0
+    sim.close()
+    full.close()
+
+
 def test_mixed_close_to_plain_accurate():
     b = ic.plummer(32_768, seed=6)
     plain = Simulation("accurate", "fp64", theta=0.5, eps=0.01, leaf_cap=16)
