@@ -58,8 +58,18 @@ __global__ void nint_kernel(const int8_t* __restrict__ dlev, int64_t n, int leaf
         if (c > 0) deep = static_cast<unsigned>(top + 1);
         if (mb >= levels) deep = kDepthOverfull;
     }
+    // block maximum, then one atomic per block, skipped when it cannot raise
+    // the value (one hot address: unconditional atomics cost more than the pass)
+    __shared__ unsigned warp_max[32];
     deep = __reduce_max_sync(0xffffffffu, deep);
-    if ((threadIdx.x & 31) == 0 && deep) atomicMax(deepest, static_cast<unsigned long long>(deep));
+    if ((threadIdx.x & 31) == 0) warp_max[threadIdx.x >> 5] = deep;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned v = threadIdx.x < (blockDim.x >> 5) ? warp_max[threadIdx.x] : 0u;
+        v = __reduce_max_sync(0xffffffffu, v);
+        if (threadIdx.x == 0 && v > *reinterpret_cast<volatile unsigned long long*>(deepest))
+            atomicMax(deepest, static_cast<unsigned long long>(v));
+    }
 }
 
 // Walk groups from the children of one cell holding more than G bodies:
