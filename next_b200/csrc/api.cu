@@ -142,6 +142,7 @@ struct next_handle {
     int sys_bits = 0;                 // bits of the system number above the octant digits
     int key_bits = 63;                // sorted key bits
     bool depth_decided = false;
+    bool cube_fresh = false;          // the last kick-drift wrote the root cube (one system)
     int64_t builds = 0;               // tree builds enqueued
     int64_t depth_seen = 0;           // the build whose depth report was last acted on
     bool pot_valid = false;
@@ -317,7 +318,10 @@ int build(next_handle* h, std::vector<int>* evs) {
     int rc0 = record(h, evs);
     if (rc0) return rc0;
     ++h->builds;
-    NB_TRY(launch_root_cubes(src, n, h->sys, h->d_offsets, h->partial, kReduceMax, h->tickets + 0, h->st), "root cube");
+    if (!h->cube_fresh)
+        NB_TRY(launch_root_cubes(src, n, h->sys, h->d_offsets, h->partial, kReduceMax, h->tickets + 0, h->st),
+               "root cube");
+    h->cube_fresh = false;
     NB_TRY(launch_keys(src, h->sysid, n, h->sys, h->keys, h->idx, h->st), "keys");
     rc0 = record(h, evs);
     if (rc0) return rc0;
@@ -459,6 +463,16 @@ int set_dt(next_handle* h, double dt) {
     return NEXT_OK;
 }
 
+// The opening half-kick and the drift; with one system the same pass boxes
+// the new positions, and the next build takes that root cube.
+cudaError_t kick_drift_step(next_handle* h, const Bodies& bd) {
+    if (h->sys.n != 1) return launch_kick_drift(bd, h->n, h->dts, h->err, h->st);
+    const cudaError_t e = launch_kick_drift_box(bd, h->n, h->dts, h->err, h->partial, kReduceMax, h->tickets + 0,
+                                                h->sys.cube, h->st);
+    h->cube_fresh = e == cudaSuccess;
+    return e;
+}
+
 // One eager step.  With evs, events bracket the stages for timing.
 int step_once(next_handle* h, bool sync_checked) {
     const bool reuse = h->prm.reuse_forces && h->forces_valid;
@@ -471,7 +485,7 @@ int step_once(next_handle* h, bool sync_checked) {
         if (rc) return rc;
     }
     Bodies bd = h->cur_bodies();
-    NB_TRY(launch_kick_drift(bd, h->n, h->dts, h->err, h->st), "kick-drift");
+    NB_TRY(kick_drift_step(h, bd), "kick-drift");
     rc = forces(h, false, E);
     if (rc) return rc;
     bd = h->cur_bodies();
@@ -511,7 +525,7 @@ int capture_step(next_handle* h) {
     h->capturing = true;
     h->cap_events.clear();
     std::vector<int> unused;
-    cudaError_t e = launch_kick_drift(bd, h->n, h->dts, h->err, h->st);
+    cudaError_t e = kick_drift_step(h, bd);
     if (e == cudaSuccess) rc = forces(h, false, &unused);
     h->capturing = false;
     h->graph_ev[parity] = h->cap_events;
@@ -771,6 +785,7 @@ int next_upload_systems(next_handle* h, int64_t n_systems, const int64_t* offset
         NB_TRY(cudaMemcpyAsync(h->sysid, sid.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, h->st), "system ids");
         NB_TRY(cudaStreamSynchronize(h->st), "sync");
     }
+    h->cube_fresh = false;
     const double* lanes[7] = {x, y, z, vx, vy, vz, m};
     for (int c = 0; c < 7; ++c)
         NB_TRY(cudaMemcpyAsync(h->stage + c * n, lanes[c], sizeof(double) * n, cudaMemcpyHostToDevice, h->st), "upload");
@@ -871,7 +886,7 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
         if (rc) return rc;
     }
     Bodies bd = h->cur_bodies();
-    NB_TRY(launch_kick_drift(bd, h->n, h->dts, h->err, h->st), "kick-drift");
+    NB_TRY(kick_drift_step(h, bd), "kick-drift");
     // the positions are final: their copies out run beside the force phase
     // (the gather into caller order precedes the re-sort in stream order)
     const double* pos[3] = {bd.x, bd.y, bd.z};

@@ -4,6 +4,7 @@
 // Built with -fmad=false: v += a*(dt/2) and x += v*dt round the product and
 // the sum separately, as the reference's loops do (src/gravity/step.h:120-122,
 // 143-145), so reference-mode trajectories match it bit for bit.
+#include "box.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -35,6 +36,48 @@ __global__ void kick_drift_kernel(Bodies b, int64_t n, const double* __restrict_
     vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
     b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
     b.x[i] += vx * dt; b.y[i] += vy * dt; b.z[i] += vz * dt;
+}
+
+// The same kick-drift over a grid-stride loop that also boxes the drifted
+// positions: the last block to finish folds the block boxes into the root
+// cube the next build needs (one system), saving the build a pass over x, y, z.
+__global__ void __launch_bounds__(kBoxThreads)
+kick_drift_box_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err, double* __restrict__ partial,
+                      unsigned int* ticket, double4* cube) {
+    if (*err & kErrAbort) return;
+    const double dt = dts[0], half = dts[1];
+    double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+        vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
+        b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
+        const double px = b.x[i] + vx * dt, py = b.y[i] + vy * dt, pz = b.z[i] + vz * dt;
+        b.x[i] = px; b.y[i] = py; b.z[i] = pz;
+        lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
+        lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
+        lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
+    }
+    block_minmax3(lo, hi);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) { partial[6 * blockIdx.x + a] = lo[a]; partial[6 * blockIdx.x + 3 + a] = hi[a]; }
+        __threadfence();
+        last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double l2[3] = {1e30, 1e30, 1e30}, h2[3] = {-1e30, -1e30, -1e30};
+    for (int k = threadIdx.x; k < gridDim.x; k += blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            l2[a] = fmin(l2[a], __ldcg(partial + 6 * k + a));
+            h2[a] = fmax(h2[a], __ldcg(partial + 6 * k + 3 + a));
+        }
+    block_minmax3(l2, h2);
+    if (threadIdx.x == 0) {
+        *cube = cube_from_box(l2, h2);
+        *ticket = 0u;
+    }
 }
 
 __global__ void kick_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err) {
@@ -221,6 +264,16 @@ cudaError_t launch_gather_bodies(const Bodies& src, const Bodies& dst, const uin
 cudaError_t launch_kick_drift(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
     kick_drift_kernel<<<grid_for(n, 256), 256, 0, st>>>(b, n, dts, err);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_kick_drift_box(const Bodies& b, int64_t n, const double* dts, const int* err, double* partial,
+                                  int partial_blocks, unsigned int* ticket, double4* cube, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    unsigned blocks = grid_for(n, kBoxThreads);
+    if (blocks > static_cast<unsigned>(partial_blocks)) blocks = static_cast<unsigned>(partial_blocks);
+    kick_drift_box_kernel<<<blocks, kBoxThreads, 0, st>>>(b, n, dts, err, partial, ticket, cube);
     count_launches(1);
     return cudaGetLastError();
 }

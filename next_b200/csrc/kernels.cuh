@@ -60,6 +60,9 @@ cudaError_t launch_walk_mixed(const Bodies& bd, int64_t nbodies, const Tree& t, 
 cudaError_t launch_gather_bodies(const Bodies& src, const Bodies& dst, const uint32_t* idx, int64_t n, uint32_t* inv,
                                  int* err, cudaStream_t st);
 cudaError_t launch_kick_drift(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st);
+// kick-drift that also writes the root cube of the drifted bodies (one system)
+cudaError_t launch_kick_drift_box(const Bodies& b, int64_t n, const double* dts, const int* err, double* partial,
+                                  int partial_blocks, unsigned int* ticket, double4* cube, cudaStream_t st);
 cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st);
 int reduce_blocks(int64_t n);
 cudaError_t launch_adaptive_dt(const Bodies& b, int64_t n, double base_dt, double* partial, unsigned int* ticket,
