@@ -1,9 +1,10 @@
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs: one histogram
 // pass over the keys for all digits, then one "onesweep" pass per 8-bit
 // digit.  A onesweep pass works on tiles of 256 x 15 pairs:
-//   1. load the tile, count its digits per warp (ballot peer masks, one
-//      shared add per digit group) and publish the per-digit tile counts
-//      in a status array (flag + count packed in one 32-bit word);
+//   1. load the tile, count its digits per warp (ballot peer masks, kept in
+//      shared memory for the ranking; one shared add per digit group) and
+//      publish the per-digit tile counts in a status array (flag + count
+//      packed in one 32-bit word);
 //   2. read the statuses of the 8 preceding tiles (decoupled look-back),
 //      and while those loads are in flight scan the counts and rank and
 //      scatter the tile into shared memory in digit order;
@@ -70,6 +71,7 @@ struct SortSmem {
     uint32_t warp_total[kWarps];
     uint64_t keys[kTile];
     uint32_t vals[kTile];
+    uint32_t peers[kItems][kThreads];   // the count pass's peer masks, reused by the ranking
     int tile;
 };
 
@@ -94,10 +96,11 @@ __device__ __forceinline__ uint32_t digit_peers(int dig) {
     return peers;
 }
 
-// Four resident blocks per SM (64 registers): the phases of one tile wait
-// on memory and on earlier tiles, so occupancy beats spill-free code here.
+// Three resident blocks per SM (80 registers, 69 KB of shared memory with
+// the stashed peer masks): the phases of one tile wait on memory and on
+// earlier tiles, so occupancy matters as much as instruction count here.
 #ifndef NB_SORT_MINB
-#define NB_SORT_MINB 4
+#define NB_SORT_MINB 3
 #endif
 __global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
@@ -131,6 +134,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     for (int k = 0; k < kItems; ++k) {
         const int dk = static_cast<int>((key[k] >> shift) & 0xff);
         const uint32_t peers = digit_peers(dk);
+        S.peers[k][threadIdx.x] = peers;
         if ((peers & lt) == 0) atomicAdd(&S.warp_hist[w][dk], static_cast<uint32_t>(__popc(peers)));
     }
     __syncthreads();
@@ -171,7 +175,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
         const int dk = static_cast<int>((key[k] >> shift) & 0xff);
-        const uint32_t peers = digit_peers(dk);
+        const uint32_t peers = S.peers[k][threadIdx.x];
         const uint32_t base = S.warp_hist[w][dk];
         const uint32_t pos = base + __popc(peers & lt);
         __syncwarp();
