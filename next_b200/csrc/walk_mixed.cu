@@ -54,6 +54,7 @@ constexpr int kPpCap = 32 + 32 * kPpChunk;
 
 struct WarpLists {
     float4 stage[3 * 32];
+    double gc[4];                // FP64 group centre, read back at each staging
     int pc[kPcCap];
     int pp[kPpCap];
 };
@@ -67,6 +68,12 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
     *total = __shfl_sync(0xffffffffu, inc, 31);
     return inc - v;
 }
+
+// The walk runs at its register cap (6 blocks of 4 warps per SM): the FP64
+// group centre is read back from shared memory at each staging rather than
+// held in six registers across the evaluation loops (fewer spills, ~1 %).
+// The volatile read keeps the compiler from hoisting it back into registers.
+__device__ __forceinline__ double vld(const double& v) { return *reinterpret_cast<const volatile double*>(&v); }
 
 struct Target {
     float tx, ty, tz;
@@ -296,6 +303,47 @@ __device__ __forceinline__ void eval_batch_packed(const float4* stage, int count
     kahan_add(T.az, T.cz, sz.x + sz.y);
 }
 
+// Stage up to 32 cells of `list` (one per lane) as a packed batch: pairs of
+// entries interleaved field by field, 5 float4 per pair; lanes past `count`
+// stage zero-mass entries.  Positions are FP64 COM minus the FP64 group
+// centre, rounded to FP32.
+template <bool QUAD>
+__device__ __forceinline__ void stage_pc_packed(float4* stage, const int* list, int count, const Tree& t, double gcx,
+                                                double gcy, double gcz, float G, int lane) {
+    float* f = reinterpret_cast<float*>(stage + 5 * (lane >> 1)) + (lane & 1);
+    float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (lane < count) {
+        const int node = list[lane];
+        const double4 c = t.com[node];
+        v[0] = static_cast<float>(c.x - gcx);
+        v[1] = static_cast<float>(c.y - gcy);
+        v[2] = static_cast<float>(c.z - gcz);
+        v[3] = static_cast<float>(G * c.w);
+        if (QUAD) {
+            const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
+            v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+}
+
+// Stage up to 32 bodies of `list` as a packed batch, 2 float4 per pair.
+__device__ __forceinline__ void stage_pp_packed(float4* stage, const int* list, int count, const Bodies& bd,
+                                                double gcx, double gcy, double gcz, float G, int lane) {
+    float* f = reinterpret_cast<float*>(stage + 2 * (lane >> 1)) + (lane & 1);
+    float v[4] = {0, 0, 0, 0};
+    if (lane < count) {
+        const int j = list[lane];
+        v[0] = static_cast<float>(bd.x[j] - gcx);
+        v[1] = static_cast<float>(bd.y[j] - gcy);
+        v[2] = static_cast<float>(bd.z[j] - gcz);
+        v[3] = static_cast<float>(G * bd.m[j]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+}
+
 // Stage up to 32 cells (one per lane) and evaluate them.  PACK stages them in
 // pairs for the .f32x2 path (lanes past `count` stage zero-mass entries).
 template <bool QUAD, bool POT, bool PACK>
@@ -303,22 +351,7 @@ __device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
     if (PACK) {
-        float* f = reinterpret_cast<float*>(L.stage + 5 * (lane >> 1)) + (lane & 1);
-        float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-        if (lane < count) {
-            const int node = list[lane];
-            const double4 c = t.com[node];
-            v[0] = static_cast<float>(c.x - gcx);
-            v[1] = static_cast<float>(c.y - gcy);
-            v[2] = static_cast<float>(c.z - gcz);
-            v[3] = static_cast<float>(G * c.w);
-            if (QUAD) {
-                const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
-                v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+        stage_pc_packed<QUAD>(L.stage, list, count, t, gcx, gcy, gcz, G, lane);
         __syncwarp();
         eval_batch_packed<5, true, QUAD>(L.stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
@@ -345,17 +378,7 @@ __device__ __forceinline__ void eval_pp(WarpLists& L, const int* list, int count
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
     if (PACK) {
-        float* f = reinterpret_cast<float*>(L.stage + 2 * (lane >> 1)) + (lane & 1);
-        float v[4] = {0, 0, 0, 0};
-        if (lane < count) {
-            const int j = list[lane];
-            v[0] = static_cast<float>(bd.x[j] - gcx);
-            v[1] = static_cast<float>(bd.y[j] - gcy);
-            v[2] = static_cast<float>(bd.z[j] - gcz);
-            v[3] = static_cast<float>(G * bd.m[j]);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+        stage_pp_packed(L.stage, list, count, bd, gcx, gcy, gcz, G, lane);
         __syncwarp();
         eval_batch_packed<2, false, false>(L.stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
@@ -406,7 +429,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
         if (static_cast<int64_t>(grp.x) + nt <= own_lo || grp.x >= own_hi) continue;
         const int64_t own_first = grp.x > own_lo ? grp.x : own_lo;
         const int64_t own_end = static_cast<int64_t>(grp.x) + nt < own_hi ? static_cast<int64_t>(grp.x) + nt : own_hi;
-        const unsigned long long own_nt = static_cast<unsigned long long>(own_end - own_first);
+        const unsigned own_nt = static_cast<unsigned>(own_end - own_first);
         // Groups of at most 16 bodies are evaluated by 2, 4, ... warp slices,
         // each taking a share of every list batch; slices are summed at the end.
         int nslices = 1;
@@ -439,7 +462,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
         int sp = 1, pc_n = 0, pp_n = 0;
         if (lane == 0) stack[0] = grp.z;
         bool failed = false;
-        unsigned long long g_pp = 0, g_pc = 0;
+        unsigned g_pp = 0, g_pc = 0;
+        if (lane == 0) { L.gc[0] = gcx; L.gc[1] = gcy; L.gc[2] = gcz; }
         __syncwarp();
         while (sp > 0) {
             const int nb = sp < 32 ? sp : 32;
@@ -480,7 +504,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
             if (pc_n >= 32) {
-                eval_pc<QUAD, POT, kPack>(L, L.pc, 32, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
+                eval_pc<QUAD, POT, kPack>(L, L.pc, 32, t, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane);
                 g_pc += 32;
                 pc_n -= 32;
                 const int v = lane < pc_n ? L.pc[32 + lane] : 0;
@@ -501,7 +525,7 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
                 __syncwarp();
                 int head = 0;
                 while (pp_n - head >= 32) {
-                    eval_pp<SOFT, POT, kPack>(L, L.pp + head, 32, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane);
+                    eval_pp<SOFT, POT, kPack>(L, L.pp + head, 32, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane);
                     g_pp += 32;
                     head += 32;
                 }
@@ -518,8 +542,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrStack);
             continue;
         }
-        if (pc_n > 0) { eval_pc<QUAD, POT, kPack>(L, L.pc, pc_n, t, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
-        if (pp_n > 0) { eval_pp<SOFT, POT, kPack>(L, L.pp, pp_n, bd, gcx, gcy, gcz, G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
+        if (pc_n > 0) { eval_pc<QUAD, POT, kPack>(L, L.pc, pc_n, t, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
+        if (pp_n > 0) { eval_pp<SOFT, POT, kPack>(L, L.pp, pp_n, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
         double fx = static_cast<double>(T.ax) - static_cast<double>(T.cx);
         double fy = static_cast<double>(T.ay) - static_cast<double>(T.cy);
         double fz = static_cast<double>(T.az) - static_cast<double>(T.cz);
@@ -536,8 +560,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             bd.az[i] = fz;
             if (POT && bd.pot) bd.pot[i] = fp;
         }
-        npp += g_pp * own_nt;
-        npc += g_pc * own_nt;
+        npp += static_cast<unsigned long long>(g_pp) * own_nt;
+        npc += static_cast<unsigned long long>(g_pc) * own_nt;
     }
     if (lane == 0) {
         if (npp) atomicAdd(stats + 0, npp);
