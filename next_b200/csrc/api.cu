@@ -156,6 +156,10 @@ struct next_handle {
     // graphs: one captured KDK step per buffer parity
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     int64_t graph_kernels[2] = {0, 0};
+    // next_step_host: force phase + closing kick per buffer parity (its
+    // kick-drift and position export run eagerly in front of the replay)
+    cudaGraphExec_t fgraph[2] = {nullptr, nullptr};
+    int64_t fgraph_kernels[2] = {0, 0};
     // events recorded inside each graph (build start, after keys, after sort,
     // after build, after walk) so a timed replay reports its stages
     std::vector<cudaEvent_t> graph_ev[2];
@@ -207,6 +211,7 @@ void free_tree(next_handle* h) {
 void drop_graphs(next_handle* h) {
     for (int p = 0; p < 2; ++p) {
         if (h->graph[p]) { cudaGraphExecDestroy(h->graph[p]); h->graph[p] = nullptr; }
+        if (h->fgraph[p]) { cudaGraphExecDestroy(h->fgraph[p]); h->fgraph[p] = nullptr; }
         for (cudaEvent_t ev : h->graph_ev[p]) cudaEventDestroy(ev);
         h->graph_ev[p].clear();
     }
@@ -509,10 +514,13 @@ int step_once(next_handle* h, bool sync_checked) {
     return NEXT_OK;
 }
 
-// Capture kick-drift + force phase + kick for the current buffer parity.
-int capture_step(next_handle* h) {
+// Capture kick-drift + force phase + kick for the current buffer parity
+// (with_kick_drift), or only the force phase + kick into the next_step_host
+// graph of that parity.
+int capture_graph(next_handle* h, bool with_kick_drift) {
     const int parity = h->cur;
-    if (h->graph[parity]) return NEXT_OK;
+    cudaGraphExec_t* slot = with_kick_drift ? &h->graph[parity] : &h->fgraph[parity];
+    if (*slot) return NEXT_OK;
     const bool saved_timing = h->timing;
     h->timing = false;
     const int saved_cur = h->cur;
@@ -524,11 +532,12 @@ int capture_step(next_handle* h) {
     Bodies bd = h->cur_bodies();
     h->capturing = true;
     h->cap_events.clear();
+    // stage-timing events only in the next_steps graph
     std::vector<int> unused;
-    cudaError_t e = kick_drift_step(h, bd);
-    if (e == cudaSuccess) rc = forces(h, false, &unused);
+    cudaError_t e = with_kick_drift ? kick_drift_step(h, bd) : cudaSuccess;
+    if (e == cudaSuccess) rc = forces(h, false, with_kick_drift ? &unused : nullptr);
     h->capturing = false;
-    h->graph_ev[parity] = h->cap_events;
+    if (with_kick_drift) h->graph_ev[parity] = h->cap_events;
     h->cap_events.clear();
     if (e == cudaSuccess && rc == NEXT_OK) {
         bd = h->cur_bodies();
@@ -538,13 +547,13 @@ int capture_step(next_handle* h) {
     cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
     const int64_t captured = launches_so_far() - launches_before;
     count_launches(static_cast<int>(-captured));   // captured, not launched
-    h->graph_kernels[parity] = captured;
+    (with_kick_drift ? h->graph_kernels : h->fgraph_kernels)[parity] = captured;
     h->cur = saved_cur;
     h->timing = saved_timing;
     if (rc) { if (g) cudaGraphDestroy(g); return rc; }
     if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(h, e, "capture"); }
     if (e2 != cudaSuccess) return cuda_fail(h, e2, "end capture");
-    e = cudaGraphInstantiate(&h->graph[parity], g, 0);
+    e = cudaGraphInstantiate(slot, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(h, e, "graph instantiate");
     return NEXT_OK;
@@ -881,6 +890,13 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
         NB_TRY(cudaStreamCreateWithFlags(&h->st_out, cudaStreamNonBlocking), "export stream");
         NB_TRY(cudaEventCreateWithFlags(&h->ev_out, cudaEventDisableTiming), "export event");
     }
+    // with mixed precision the force phase and the closing kick replay a
+    // captured graph (one per buffer parity), as next_steps' steps do
+    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces;
+    if (use_graph && !h->fgraph[h->cur] && h->forces_valid) {
+        rc = grow_if_tight(h);   // before a capture, as next_steps does
+        if (rc) return rc;
+    }
     if (!(h->prm.reuse_forces && h->forces_valid)) {
         rc = forces_checked(h, false);
         if (rc) return rc;
@@ -892,12 +908,31 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
     const double* pos[3] = {bd.x, bd.y, bd.z};
     double* pos_out[3] = {x, y, z};
     rc = export_lanes(h, pos, pos_out, 3, 0, h->st_out);
-    if (rc == NEXT_OK) rc = forces(h, false, nullptr);
-    if (rc == NEXT_OK) {
-        bd = h->cur_bodies();
-        const cudaError_t e = launch_kick(bd, h->n, h->dts, h->err, h->st);
-        if (e != cudaSuccess) rc = cuda_fail(h, e, "kick");
+    if (rc == NEXT_OK && use_graph) {
+        rc = capture_graph(h, false);
+        if (rc == NEXT_OK) {
+            const int parity = h->cur;
+            const cudaError_t e = cudaGraphLaunch(h->fgraph[parity], h->st);
+            if (e != cudaSuccess) {
+                rc = cuda_fail(h, e, "graph launch");
+            } else {
+                ++h->builds;              // the replay's build
+                count_launches(static_cast<int>(h->fgraph_kernels[parity]));
+                h->cur = 1 - h->cur;
+                h->cube_fresh = false;    // consumed by the replay's build
+                h->forces_valid = true;
+                h->pot_valid = false;
+            }
+        }
+    } else if (rc == NEXT_OK) {
+        rc = forces(h, false, nullptr);
+        if (rc == NEXT_OK) {
+            bd = h->cur_bodies();
+            const cudaError_t e = launch_kick(bd, h->n, h->dts, h->err, h->st);
+            if (e != cudaSuccess) rc = cuda_fail(h, e, "kick");
+        }
     }
+    bd = h->cur_bodies();
     const cudaError_t es = cudaStreamSynchronize(h->st_out);   // no copy into the caller's arrays outlives the call
     if (rc) return rc;
     if (es != cudaSuccess) return cuda_fail(h, es, "position copies");
@@ -946,7 +981,7 @@ int next_steps(next_handle* h, double dt, int nsteps) {
             if (rc) return rc;
             if (!h->forces_valid) continue;
         }
-        rc = capture_step(h);
+        rc = capture_graph(h, true);
         if (rc) return rc;
         const int parity = h->cur;
         std::vector<int> evs;

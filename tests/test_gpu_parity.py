@@ -319,14 +319,16 @@ def test_graph_steps_equal_eager_steps():
 @pytest.mark.parametrize("precision", ["mixed", "fp64"])
 def test_step_host_equals_upload_step_download(precision):
     """next_step_host (Step() on host arrays, positions copied back during the
-    force phase) gives the same state as next_upload + next_step + next_download."""
+    force phase, which with mixed precision replays a captured graph per buffer
+    parity) gives the same state as next_upload + next_step + next_download.
+    Four steps: both parities are captured and replayed."""
     b = ic.plummer(30_000, seed=12)
     s = Simulation("accurate", precision)
     h = Simulation("accurate", precision)
     names = ("x", "y", "z", "vx", "vy", "vz", "m")
     lanes = [np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names]
     ref = {k: np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names}
-    for _ in range(3):
+    for _ in range(4):
         s.upload_arrays([ref[k] for k in names])
         s.step(1e-3)
         s.download(ref)
