@@ -37,7 +37,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
 # capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
-WALK_DRAM_BYTES = 56.51e6
+WALK_DRAM_BYTES = 56.88e6
 SORT_BYTES_PER_BODY = 8 * 24 + 8
 
 
