@@ -1314,6 +1314,12 @@ int next_autotune(next_handle* h, next_tune_result* out) {
         for (int l : {8, 12, 16, 24})
             for (int w : {2, 4})
                 if (l <= g) cands.push_back({l, g, w});
+    // Small systems have fewer groups than the GPU has resident warps, and a
+    // walk lasts as long as its slowest group: smaller groups (split over
+    // more lane slices) put more warps to work there.
+    if (h->n <= (int64_t(1) << 18))
+        for (int l : {4, 8})
+            for (int w : {2, 4}) cands.push_back({l, 8, w});
     const Params saved_P = h->P;
     const next_params saved_prm = h->prm;
     cudaEvent_t a, b;
