@@ -188,7 +188,9 @@ int next_debug_order(next_handle* h, int64_t* perm);
 int next_debug_tree(next_handle* h, double* rows, int64_t cap, int64_t* n_rows);
 
 /* Stable LSD radix sort of (key, value) pairs on the device, the sort the
- * tree build uses: n pairs in, sorted pairs out (host arrays). */
+ * tree build uses: n pairs in, sorted pairs out (host arrays), ordered by the
+ * low key_bits bits of the keys (higher bits are carried through unchanged).
+ * NEXT_ERR_DEVICE if the sort raised its device error word. */
 int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const uint32_t* vals_in,
                     uint64_t* keys_out, uint32_t* vals_out, int key_bits);
 
@@ -198,17 +200,22 @@ int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const ui
  * mid-step.  It has no counterpart in the reference, which sorts nothing.
  *
  * Sorts n (key, value) pairs from caller-owned DEVICE buffers d_keys_in /
- * d_vals_in into caller-owned DEVICE buffers d_keys_out / d_vals_out (stable,
- * low key_bits bits significant); the inputs are left untouched and must not
- * alias the outputs.  It allocates nothing: all scratch comes from one
- * static device array sized for NEXT_SORT_NOALLOC_MAX_PAIRS pairs (about
- * 14.3 MiB, reserved on every GPU that loads it until the process exits);
- * larger n is rejected with NEXT_ERR_INVALID_ARGUMENT.  The first call on a
- * device looks up that array's address and sets the sort kernel's shared-
- * memory limit, so make it before any stream capture.  Work is queued on
- * `stream` (a cudaStream_t; NULL = default stream) of the current device and
- * the call returns after that stream has finished it.  Every call reuses the
- * same array, so calls whose GPU work overlaps race: serialise them. */
+ * d_vals_in into caller-owned DEVICE buffers d_keys_out / d_vals_out, stably
+ * by the low key_bits bits of the keys (higher bits take no part in the
+ * order and are carried through unchanged).  The inputs are left untouched;
+ * no output may overlap an input or the other output (checked byte range by
+ * byte range: NEXT_ERR_INVALID_ARGUMENT).  It allocates nothing: all scratch
+ * comes from one static device array sized for NEXT_SORT_NOALLOC_MAX_PAIRS
+ * pairs (14,844,192 bytes = 14.16 MiB, reserved on every GPU that loads the
+ * library until the process exits); larger n is rejected with
+ * NEXT_ERR_INVALID_ARGUMENT.  The first call in each CUDA context (normally
+ * once per device) looks up that array's address and sets the sort kernel's
+ * shared-memory limit, so make that first call before any stream capture.
+ * Work is queued on `stream` (a cudaStream_t; NULL = default stream) of the
+ * current device; the call reads the sort's error word back on that stream
+ * and returns after the stream has finished (NEXT_ERR_DEVICE if the sort
+ * raised an error).  Every call reuses the same array, so calls whose GPU
+ * work overlaps race: serialise them. */
 #define NEXT_SORT_NOALLOC_MAX_PAIRS 1048576
 int next_sort_pairs_noalloc(const uint64_t* d_keys_in, const uint32_t* d_vals_in, uint64_t* d_keys_out,
                             uint32_t* d_vals_out, int64_t n, int key_bits, void* stream);

@@ -1244,6 +1244,8 @@ int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const ui
     auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
     A(&k0, n); A(&k1, n); A(&v0, n); A(&v1, n); A(&scr, sort_scratch_words(n));
     bool in_alt = false;
+    // bits an earlier step left in the error word must not fail this sort
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->err, 0, sizeof(int), h->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(k0, keys_in, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, h->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(v0, vals_in, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, h->st);
     if (e == cudaSuccess) e = radix_sort_pairs(k0, v0, k1, v1, n, key_bits, scr, h->err, &in_alt, h->st);
@@ -1251,12 +1253,13 @@ int next_sort_pairs(next_handle* h, int64_t n, const uint64_t* keys_in, const ui
         e = cudaMemcpyAsync(keys_out, in_alt ? k1 : k0, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess && vals_out)
         e = cudaMemcpyAsync(vals_out, in_alt ? v1 : v0, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, h->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->h_err, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->st);
-    int bits = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&bits, h->err, sizeof(int), cudaMemcpyDeviceToHost);
+    const int bits = e == cudaSuccess ? *h->h_err : 0;
     dfree(k0); dfree(k1); dfree(v0); dfree(v1); dfree(scr);
     if (e != cudaSuccess) return cuda_fail(h, e, "sort");
     if (bits & kErrSort) return fail(h, NEXT_ERR_DEVICE, "sort look-back timeout");
+    if (bits) return fail(h, NEXT_ERR_DEVICE, "sort raised device error word " + std::to_string(bits));
     return NEXT_OK;
 }
 

@@ -34,14 +34,22 @@ constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 20;
 constexpr int kLookWindow = 8;   // earlier tiles whose status one look-back step reads
 
+// Digit mask of pass p for keys of key_bits significant bits: bits at and
+// above key_bits take no part in the ordering.
+__host__ __device__ __forceinline__ uint32_t pass_mask(int key_bits, int p) {
+    const int left = key_bits - 8 * p;
+    return left >= 8 ? 0xffu : (1u << left) - 1u;
+}
+
 __global__ void __launch_bounds__(kThreads)
-histogram_kernel(const uint64_t* __restrict__ keys, int64_t n, int passes, uint32_t* __restrict__ hist) {
+histogram_kernel(const uint64_t* __restrict__ keys, int64_t n, int key_bits, uint32_t* __restrict__ hist) {
+    const int passes = (key_bits + 7) / 8;
     __shared__ uint32_t local[8][kRadix];
     for (int i = threadIdx.x; i < 8 * kRadix; i += kThreads) (&local[0][0])[i] = 0;
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kThreads) {
         const uint64_t k = keys[i];
-        for (int p = 0; p < passes; ++p) atomicAdd(&local[p][(k >> (8 * p)) & 0xff], 1u);
+        for (int p = 0; p < passes; ++p) atomicAdd(&local[p][(k >> (8 * p)) & pass_mask(key_bits, p)], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
@@ -105,7 +113,7 @@ __device__ __forceinline__ uint32_t digit_peers(int dig) {
 __global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
-                const uint32_t* __restrict__ digit_offsets, uint32_t* status, unsigned int* tile_ticket,
+                uint32_t dmask, const uint32_t* __restrict__ digit_offsets, uint32_t* status, unsigned int* tile_ticket,
                 int* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
@@ -132,7 +140,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const int dk = static_cast<int>((key[k] >> shift) & 0xff);
+        const int dk = static_cast<int>((key[k] >> shift) & dmask);
         const uint32_t peers = digit_peers(dk);
         S.peers[k][threadIdx.x] = peers;
         if ((peers & lt) == 0) atomicAdd(&S.warp_hist[w][dk], static_cast<uint32_t>(__popc(peers)));
@@ -174,7 +182,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     // to its local slot as it is ranked.
 #pragma unroll
     for (int k = 0; k < kItems; ++k) {
-        const int dk = static_cast<int>((key[k] >> shift) & 0xff);
+        const int dk = static_cast<int>((key[k] >> shift) & dmask);
         const uint32_t peers = S.peers[k][threadIdx.x];
         const uint32_t base = S.warp_hist[w][dk];
         const uint32_t pos = base + __popc(peers & lt);
@@ -222,7 +230,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         const int i = k * kThreads + threadIdx.x;
         if (i < valid) {
             const uint64_t kk = S.keys[i];
-            const int dd = static_cast<int>((kk >> shift) & 0xff);
+            const int dd = static_cast<int>((kk >> shift) & dmask);
             const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
             if (gpos >= n) { raise_error(err, kErrIndex); continue; }
             keys_out[gpos] = kk;
@@ -265,13 +273,13 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
     if (e != cudaSuccess) return e;
     int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
     if (hblocks > 1184) hblocks = 1184;
-    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys, n, passes, hist);
+    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys, n, key_bits, hist);
     digit_offsets_kernel<<<passes, kRadix, 0, st>>>(hist, offsets);
     uint64_t* src_k = keys; uint32_t* src_v = vals;
     uint64_t* dst_k = alt_keys; uint32_t* dst_v = alt_vals;
     for (int p = 0; p < passes; ++p) {
         onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
-            src_k, src_v, dst_k, dst_v, n, 8 * p, offsets + p * kRadix,
+            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
             status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         uint64_t* tk = src_k; src_k = dst_k; dst_k = tk;
         uint32_t* tv = src_v; src_v = dst_v; dst_v = tv;
@@ -310,7 +318,7 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
     if (e != cudaSuccess) return e;
     int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
     if (hblocks > 1184) hblocks = 1184;
-    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys_in, n, passes, hist);
+    histogram_kernel<<<hblocks, kThreads, 0, st>>>(keys_in, n, key_bits, hist);
     digit_offsets_kernel<<<passes, kRadix, 0, st>>>(hist, offsets);
     const uint64_t* src_k = keys_in;
     const uint32_t* src_v = vals_in;
@@ -319,7 +327,7 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
         uint64_t* dst_k = to_out ? keys_out : alt_keys;
         uint32_t* dst_v = to_out ? vals_out : alt_vals;
         onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
-            src_k, src_v, dst_k, dst_v, n, 8 * p, offsets + p * kRadix,
+            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
             status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         src_k = dst_k;
         src_v = dst_v;

@@ -144,6 +144,7 @@ class Reference:
         L.ref_tree_export.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_int64]
         L.ref_tree_export.restype = C.c_int64
         L.ref_leaf_paths.argtypes = [C.c_int64, _d, _d, _d, _d, _u64, _i32]
+        L.ref_save_snapshot.argtypes = [C.c_int64, _d, _d, _d, _d, _d, _d, _d, _i32, C.c_int, C.c_char_p]
 
     def set_threads(self, k):
         self.lib.ref_set_threads(int(k))
@@ -184,6 +185,14 @@ class Reference:
         nn = self.lib.ref_tree_export(n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(rows, _d), cap)
         assert nn <= cap
         return rows[:nn]
+
+    def save_snapshot(self, b, path, fmt):
+        """Write `b` with the reference's SaveVTK (fmt "vtk") or SaveVTU (fmt "vtu")."""
+        n = b["x"].shape[0]
+        lanes = [_f64(b[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+        t = _i32a(b.get("type", np.zeros(n, np.int32)))
+        self.lib.ref_save_snapshot(n, *(_p(a, _d) for a in lanes), _p(t, _i32), int(fmt == "vtu"),
+                                   str(path).encode())
 
     def leaf_paths(self, b):
         n = b["x"].shape[0]

@@ -4,7 +4,8 @@
 //   -I<reference>/src -I<reference>/include -DNEXT_FP64
 // so that the #includes below pull in the unmodified reference headers
 // (src/gravity/step.h, src/gravity/octree.h, src/dt/softening.h,
-//  src/dt/adaptive.h, src/struct/particle.h, include/floatdef.h).
+//  src/dt/adaptive.h, src/struct/particle.h, include/floatdef.h, and the
+//  snapshot writers src/io/vtk_save.h, src/io/vtu_save.h).
 // The resulting oracle/_ref/libnextref.so is used by the tests as the
 // ground truth for reference-semantics parity, by tests/golden/make_golden.py
 // to produce the committed fixtures, and by bench.py as the timed CPU
@@ -12,6 +13,8 @@
 // links or loads it.
 #include "gravity/step.h"
 #include "dt/adaptive.h"
+#include "io/vtk_save.h"
+#include "io/vtu_save.h"
 
 #include <cstdint>
 #include <functional>
@@ -163,6 +166,17 @@ int ref_leaf_paths(int64_t n, const double* x, const double* y, const double* z,
         paths[i] = key;
         depth[i] = lvl;
     }
+    return 0;
+}
+
+// A snapshot written by the reference's own writers: SaveVTK
+// (src/io/vtk_save.h:21-75) or SaveVTU (src/io/vtu_save.h:22-78).
+int ref_save_snapshot(int64_t n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz,
+                      const double* m, const int* type, int vtu, const char* path) {
+    Particle p = make_particles(n, x, y, z, vx, vy, vz, m, type);
+    if (vtu) SaveVTU(p, path);
+    else SaveVTK(p, path);
     return 0;
 }
 

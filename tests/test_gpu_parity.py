@@ -75,6 +75,19 @@ def test_sort_matches_stable_sort(ref_sim, n, bits):
     np.testing.assert_array_equal(vo, vals[order])
 
 
+@pytest.mark.parametrize("n,bits", [(50_000, 12), (3841, 1), (200_000, 41)])
+def test_sort_ignores_bits_above_key_bits(ref_sim, n, bits):
+    # bits at and above key_bits take no part in the order (even those below
+    # the next multiple of 8, which the last 8-bit pass would otherwise see)
+    rng = np.random.default_rng(n * bits)
+    keys = rng.integers(0, 2 ** 63, n, dtype=np.uint64)
+    vals = rng.permutation(n).astype(np.uint32)
+    ko, vo = ref_sim.sort_pairs(keys, vals, bits)
+    order = np.argsort(keys & np.uint64((1 << bits) - 1), kind="stable")
+    np.testing.assert_array_equal(ko, keys[order])
+    np.testing.assert_array_equal(vo, vals[order])
+
+
 def test_body_order_is_stable_key_order(oracle, ref_sim):
     b = ic.plummer(50_000, seed=3)
     ref_sim.upload(b)

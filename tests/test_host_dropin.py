@@ -46,6 +46,38 @@ def test_text_loader_stops_at_first_malformed_row(tmp_path):
 
 
 @pytest.fixture(scope="module")
+def snapshot_bin(tmp_path_factory):
+    """The drop-in VTK/VTU writers (header-only, no GPU) in a small program."""
+    out = tmp_path_factory.mktemp("bin") / "save_snapshot"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-DNEXT_FP64", f"-I{HOST}",
+                    os.path.join(ROOT, "tests", "cpp", "save_snapshot.cpp"), "-o", str(out)], check=True)
+    return str(out)
+
+
+@pytest.mark.parametrize("fmt", ["vtk", "vtu"])
+def test_snapshot_bytes_equal_reference_writer(tmp_path, snapshot_bin, fmt):
+    """SaveVTK / SaveVTU write the same bytes as the reference's own writers
+    (src/io/vtk_save.h:21-75, src/io/vtu_save.h:22-78), NEXT_FP64 build."""
+    from oracle.oracle import Reference
+    rng = np.random.default_rng(31)
+    n = 1000
+    b = ic.plummer(n, seed=5)
+    b["type"] = rng.integers(0, 2, n).astype(np.int32)
+    b["m"][::97] = 0.0                                # zero masses print as "0"
+    b["x"][3], b["vy"][4] = -1.25e-7, 3.5e12          # exponent formatting
+    raw = tmp_path / "bodies.bin"
+    with open(raw, "wb") as f:
+        for k in ("x", "y", "z", "vx", "vy", "vz", "m"):
+            f.write(np.ascontiguousarray(b[k], dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(b["type"], dtype=np.int32).tobytes())
+    mine, ref = tmp_path / f"mine.{fmt}", tmp_path / f"ref.{fmt}"
+    subprocess.run([snapshot_bin, str(raw), str(n), fmt, str(mine)], check=True)
+    Reference().save_snapshot(b, ref, fmt)
+    assert mine.read_bytes() == ref.read_bytes()
+    assert mine.stat().st_size > 60 * n
+
+
+@pytest.fixture(scope="module")
 def dropin_bin(tmp_path_factory):
     out = tmp_path_factory.mktemp("bin") / "dropin_step"
     subprocess.run(["g++", "-O2", "-std=c++17", f"-I{HOST}", os.path.join(ROOT, "tests", "cpp", "dropin_step.cpp"),
