@@ -38,7 +38,22 @@ FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
 # capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
 WALK_DRAM_BYTES = 56.88e6
-SORT_BYTES_PER_BODY = 8 * 24 + 8
+L2_BYTES = 126 * 2 ** 20
+
+
+def sort_passes(key_levels, n_systems):
+    """Onesweep passes of the key sort: ceil(key_bits / 8), key_bits = the
+    octant digits kept (3 per level; all 63 bits below the system number at
+    full depth) plus the bits of the system number."""
+    sys_bits = 0 if n_systems <= 1 else int(math.ceil(math.log2(n_systems)))
+    full = min(21, (63 - sys_bits) // 3)
+    base = 63 - sys_bits if key_levels >= full else 3 * key_levels
+    return -(-(base + sys_bits) // 8)
+
+
+def sort_bytes_per_body(passes):
+    # each pass reads and writes a (u64 key, u32 index) pair; the histogram pass reads the keys once
+    return passes * 24 + 8
 
 
 def env_rank():
@@ -159,6 +174,15 @@ def run_reference_arm(args):
         b = R.step(b, WORKLOAD["dt"], 1)
     t = time.perf_counter() - t0
     value = WORKLOAD["n"] * steps / t
+    # the reference's as-shipped forces on 4096 seeded bodies of the initial
+    # state against FP64 direct summation (CPU oracle) with the workload's eps
+    from oracle.oracle import Oracle
+    idx = np.random.default_rng(12345).choice(WORKLOAD["n"], 4096, replace=False)
+    a = R.accel_sample(bodies, idx)
+    d = Oracle().direct(bodies, idx, eps=WORKLOAD["eps"])
+    ferr = force_error(a, d, np.arange(idx.shape[0]))
+    ferr["versus"] = (f"FP64 direct summation with Plummer eps {WORKLOAD['eps']} on 4096 sampled bodies of the "
+                      f"initial state (the reference's own softening differs)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
@@ -168,7 +192,9 @@ def run_reference_arm(args):
                    "physics": "reference as shipped", "l2": "host run"},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
                          "sample": f"{steps} timed Step() call(s) on the full system after "
-                                   f"{min(args.warmup, 1)} warm-up; bounded so the run ends in minutes"},
+                                   f"{min(args.warmup, 1)} warm-up; bounded so the run ends in minutes",
+                         "force_error": ferr},
+        "force_error": ferr,
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -264,6 +290,65 @@ def plain_fp64_leg(bodies, offsets, cfg, device, steps, idx):
             "structure": "single-system plain FP64 step looped over 16 sampled systems (device time summed)"}
 
 
+def ref_physics_leg(bodies, cfg, device, steps, idx, d_direct, cpu_accel):
+    """The drop-in default: reference physics (adaptive softening, the
+    reference's opening test and quadrupole) in plain FP64 on the GPU -- what
+    Step() and the `next` CLI run -- timed over `steps` KDK steps."""
+    from next_b200.native import Simulation
+    p = Simulation("reference", "fp64", device=device)
+    p.upload(bodies)
+    a = p.accel()
+    err = force_error(a, d_direct, idx) if d_direct is not None else None
+    parity = None
+    if cpu_accel is not None:
+        num = np.sqrt(sum((a[c][idx] - cpu_accel[c]) ** 2 for c in ("ax", "ay", "az")))
+        den = np.sqrt(sum(cpu_accel[c] ** 2 for c in ("ax", "ay", "az")))
+        parity = float(np.max(num / den))
+    p.step(cfg["dt"])
+    p.sync()
+    p.reset_timers()
+    p.set_timing(True)
+    for _ in range(steps):
+        p.flush_l2()
+        p.step(cfg["dt"])
+    p.sync()
+    st = p.stats()
+    p.close()
+    n = bodies["x"].shape[0]
+    return {"value": n * steps / (st["ms_step"] * 1e-3), "unit": "particle-steps/s", "steps": steps,
+            "ms_per_step": st["ms_step"] / steps, "force_error": err,
+            "max_rel_diff_vs_reference_cpu": parity,
+            "physics": "reference (as the CPU arm: adaptive softening, half-width theta 0.5, its quadrupole)",
+            "structure": "one thread per body, one body per leaf, two tree builds per step (step.h:113,164)"}
+
+
+def large_sort_leg(cfg, device, n=8_388_608, steps=3):
+    """The key sort at a size whose ping-pong buffers exceed the 126 MB L2:
+    the same workload at n bodies, sort stage of `steps` eager steps."""
+    from next_b200 import ic
+    from next_b200.native import Simulation
+    b = ic.uniform_sphere(n, seed=cfg["seed"])
+    sim = Simulation("accurate", "mixed", theta=cfg["theta"], eps=cfg["eps"], device=device)
+    sim.upload(b)
+    sim.steps(cfg["dt"], 2)
+    sim.sync()
+    sim.reset_timers()
+    sim.set_timing(True)
+    for _ in range(steps):
+        sim.flush_l2()
+        sim.step(cfg["dt"])
+    sim.sync()
+    st = sim.stats()
+    sim.close()
+    passes = sort_passes(st["key_levels"], 1)
+    ms = st["ms_sort"] / steps
+    gbs = sort_bytes_per_body(passes) * n / (ms * 1e-3) / 1e9
+    peak = measured_peaks().get("hbm_gbs")
+    return {"n_bodies": n, "passes": passes, "bytes_per_body": sort_bytes_per_body(passes), "ms": ms,
+            "gbs": gbs, "frac": gbs / peak if peak else None,
+            "note": "ping-pong buffers of 24 B/body x 2 exceed the L2: an HBM figure"}
+
+
 def run_ours(args):
     rank, world, local = env_rank()
     from next_b200.native import Simulation, fp32_peak, load
@@ -283,12 +368,11 @@ def run_ours(args):
     bodies, offsets = make_bodies(W)
     sharded = world > 1 and offsets is None      # one system over all ranks (force all-gather)
     if world > 1 and offsets is not None:
-        # independent systems: each rank integrates its own slice of them, no collective
-        s0 = rank * (len(offsets) - 1) // world
-        s1 = (rank + 1) * (len(offsets) - 1) // world
-        sl = slice(offsets[s0], offsets[s1])
-        bodies = {k: v[sl] for k, v in bodies.items()}
-        offsets = offsets[s0:s1 + 1] - offsets[s0]
+        # independent systems: each rank integrates whole systems, balanced by
+        # N log N work (the same split on every rank), no collective
+        from next_b200.dist import select_systems, split_systems
+        mine = split_systems(np.diff(offsets), world)[rank]
+        bodies, offsets = select_systems(bodies, offsets, mine)
     n = bodies["x"].shape[0]
     knobs = dict(leaf_cap=args.leaf_cap, group_cap=args.group_cap, walk_warps=args.walk_warps,
                  walk_stack=args.walk_stack)
@@ -317,8 +401,10 @@ def run_ours(args):
     # force error vs FP64 direct summation at the current positions
     idx = np.random.default_rng(12345).choice(n, min(4096, n), replace=False)
     a_mixed = sim.accel()
+    d_direct = None
     if offsets is None:
-        err_mixed = force_error(a_mixed, sim.direct_accel(idx), idx)
+        d_direct = sim.direct_accel(idx)
+        err_mixed = force_error(a_mixed, d_direct, idx)
     else:
         now = dict(bodies)
         now.update(sim.download())          # the direct sums must see the current positions
@@ -388,6 +474,21 @@ def run_ours(args):
     fp64 = None
     if rank == 0 and not args.skip_fp64:
         fp64 = plain_fp64_leg(bodies, offsets, W, local, max(1, args.fp64_steps), idx)
+    # the reference's as-shipped forces on the same sampled bodies, same state
+    cpu_accel = None
+    now = None
+    if rank == 0 and offsets is None and d_direct is not None and not args.skip_cpu and n <= 2_000_000:
+        from oracle.oracle import Reference
+        now = dict(bodies)
+        now.update(sim.download())
+        cpu_accel = Reference().accel_sample(now, idx)
+    refphys = None
+    if rank == 0 and offsets is None and world == 1 and not args.skip_fp64:
+        refphys = ref_physics_leg(now if now is not None else bodies, W, local, max(1, args.fp64_steps), idx,
+                                  d_direct if now is not None else None, cpu_accel)
+    big_sort = None
+    if rank == 0 and world == 1 and args.config == "c2" and not args.skip_large_sort:
+        big_sort = large_sort_leg(W, local)
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if rank == 0 and not args.skip_e2e and offsets is None and world == 1:
@@ -414,6 +515,10 @@ def run_ours(args):
     if rank == 0 and not args.skip_cpu:
         if offsets is None and n <= 2_000_000:
             cpu = time_cpu_reference(bodies, W["dt"], args.cpu_budget)
+            if cpu_accel is not None:
+                cpu["force_error"] = force_error(cpu_accel, d_direct, np.arange(idx.shape[0]))
+                cpu["force_error"]["versus"] = (f"FP64 direct summation with Plummer eps {W['eps']} on the same "
+                                                f"{idx.shape[0]} sampled bodies (the reference's own softening differs)")
         else:
             cpu = {"skipped": "one reference Step() at this size takes minutes on the host; see the c2 line"}
     prm = sim.get_params()
@@ -423,6 +528,9 @@ def run_ours(args):
             dist.destroy_process_group()
         return 0
     peaks = measured_peaks()
+    passes = sort_passes(st["key_levels"], 1 if offsets is None else len(offsets) - 1)
+    sort_bpb = sort_bytes_per_body(passes)
+    sort_gbs = sort_bpb * total_bodies / (st["ms_sort"] / args.steps * 1e-3) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
@@ -441,6 +549,7 @@ def run_ours(args):
                         "versus": "FP64 direct summation on seeded bodies"},
         "fp64_gpu": fp64,
         "speedup_vs_fp64_gpu": value / fp64["value"] if fp64 and world == 1 else None,
+        "ref_physics_fp64_gpu": refphys,
         "eager_value": total_bodies * args.steps / (eager_ms * 1e-3) if eager_ms else None,
         "step_launch": "one CUDA-graph replay per KDK step (captured kick-drift + force phase + kick)",
         "interactions_per_s": (st["pp_interactions"] + st["pc_interactions"]) / (st["ms_walk"] * 1e-3),
@@ -448,12 +557,15 @@ def run_ours(args):
         "pp_fraction": st["pp_interactions"] / max(1, st["pp_interactions"] + st["pc_interactions"]),
         "pp_interactions_per_s": st["pp_interactions"] / (st["ms_walk"] * 1e-3),
         "pc_interactions_per_s": st["pc_interactions"] / (st["ms_walk"] * 1e-3),
-        # the key sort's algorithmic traffic: 8 passes x (12 B read + 12 B written) + the
-        # 8-byte histogram read, per body, over the bench's own sort stage time
-        "sort_hbm": {"bytes_per_body": SORT_BYTES_PER_BODY,
-                     "gbs": SORT_BYTES_PER_BODY * total_bodies / (st["ms_sort"] / args.steps * 1e-3) / 1e9,
-                     "frac": SORT_BYTES_PER_BODY * total_bodies / (st["ms_sort"] / args.steps * 1e-3) / 1e9 / peaks["hbm_gbs"]
-                     if peaks.get("hbm_gbs") else None},
+        # the key sort's algorithmic traffic: passes x (12 B read + 12 B written) + the
+        # 8-byte histogram read, per body, over the bench's own sort stage time;
+        # passes = ceil(key bits / 8) of this run's keys (trimmed to the tree depth)
+        "sort_hbm": {"passes": passes, "key_levels": st["key_levels"], "bytes_per_body": sort_bpb,
+                     "gbs": sort_gbs, "frac": sort_gbs / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+                     "l2_resident": 2 * 24 * total_bodies < L2_BYTES,
+                     "note": ("ping-pong buffers fit in the L2: not an HBM figure (see sort_hbm_large)"
+                              if 2 * 24 * total_bodies < L2_BYTES else "buffers exceed the L2")},
+        "sort_hbm_large": big_sort,
         "tree": {"nodes": st["n_nodes"], "internal": st["n_internal"], "groups": st["n_groups"] - st["n_systems"],
                  "bodies_per_group": n / max(1, st["n_groups"] - st["n_systems"]), "max_walk_stack": st["max_stack"]},
         "stage_ms_per_step": {"build": st["ms_build"] / args.steps, "sort": st["ms_sort"] / args.steps,
@@ -490,6 +602,7 @@ def main():
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-large-sort", action="store_true")
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS), help="workload (default c2, the metric's)")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--n", type=int, default=None, help="override the body count of a single-system config")

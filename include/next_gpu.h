@@ -99,7 +99,8 @@ typedef struct next_stats {
     double ms_other;         /* ... kick/drift and the rest */
     int64_t walk_launches;   /* walks timed */
     int32_t key_levels;      /* octant levels in the keys of the last build (21 = full depth) */
-    int32_t reserved;
+    int32_t recoveries;      /* graph-replayed steps (next_steps) that overflowed a capacity and were
+                                finished by re-running their force phase and closing kick */
 } next_stats;
 
 typedef struct next_handle next_handle;
@@ -138,7 +139,11 @@ int next_download(next_handle* h, double* x, double* y, double* z,
 int next_step(next_handle* h, double dt);
 
 /* nsteps steps of fixed dt; with mixed precision each step is one replay of a
- * captured CUDA graph. */
+ * captured CUDA graph.  The device error word is read every 64 replays and at
+ * the end; a replay that overflowed a capacity (tree, walk stack) is finished
+ * as next_step would finish it -- capacity grown, force phase and closing kick
+ * re-run -- and the steps after it are taken again, so the result equals the
+ * same steps taken one by one (next_stats.recoveries counts such replays). */
 int next_steps(next_handle* h, double dt, int nsteps);
 
 /* The reference's Step(ParticleSystem&, dt) on host arrays (src/gravity/
@@ -176,6 +181,17 @@ int next_sync(next_handle* h);
  * 3 bits from bit 62 down) of the uploaded bodies in the caller's order, and
  * the root cube (cx, cy, cz, half-width) of step.h:69-100. */
 int next_debug_keys(next_handle* h, uint64_t* keys, double* cube4);
+
+/* Test support: the device's reference softening law nextSoftening
+ * (src/dt/softening.h:21-35), as the reference-physics walk evaluates it, on
+ * k (size, mass, dist) triples. */
+int next_debug_softening(int device, int64_t k, const double* size, const double* mass, const double* dist,
+                         double* out);
+
+/* Test support: sets the tree's capacity to cap_internal internal cells and
+ * from then on grows it only when a build overflows it (not ahead of need),
+ * so that tests can make a graph-replayed step overflow. */
+int next_debug_fix_tree_capacity(next_handle* h, int64_t cap_internal);
 
 /* Stable key order of the last build: perm[p] = caller's index of the p-th
  * body in key order. */

@@ -113,6 +113,7 @@ struct next_handle {
     double* diag = nullptr;                // 8
     int* changed = nullptr;
     float* fma_out = nullptr;
+    unsigned int* done = nullptr;          // closing kicks completed by graph replays (next_steps)
 
     // pinned host scalars
     double* h_dts = nullptr;
@@ -120,6 +121,7 @@ struct next_handle {
     int* h_flags = nullptr;                // upload check: changed, non-finite, negative mass
     int64_t* h_counts = nullptr;           // internal, nodes, groups
     unsigned long long* h_stats = nullptr;
+    unsigned int* h_done = nullptr;
 
     // direct summation scratch
     int64_t* d_targets = nullptr;
@@ -147,6 +149,8 @@ struct next_handle {
     int64_t depth_seen = 0;           // the build whose depth report was last acted on
     bool pot_valid = false;
     bool sorted_in_alt = false;
+    int64_t recoveries = 0;           // graph replays that overflowed and were finished eagerly
+    bool fixed_tree_cap = false;      // test support: grow the tree only on overflow
 
     // sharding over ranks: every rank holds all bodies, computes the forces of
     // its share [rank*chunk, (rank+1)*chunk) and all-gathers the rest
@@ -541,7 +545,7 @@ int capture_graph(next_handle* h, bool with_kick_drift) {
     h->cap_events.clear();
     if (e == cudaSuccess && rc == NEXT_OK) {
         bd = h->cur_bodies();
-        e = launch_kick(bd, h->n, h->dts, h->err, h->st);
+        e = launch_kick(bd, h->n, h->dts, h->err, h->st, with_kick_drift ? h->done : nullptr);
     }
     h->builds = builds_before;
     cudaError_t e2 = cudaStreamEndCapture(h->st, &g);
@@ -622,7 +626,7 @@ int add_graph_timing(next_handle* h, int parity, const std::vector<int>& evs) {
 // Grow capacities that the last build came close to (before a graph capture).
 int grow_if_tight(next_handle* h) {
     const int64_t internal = h->h_counts[0], nodes = h->h_counts[1];
-    if (4 * internal > 3 * h->t.cap_int || 4 * nodes > 3 * h->t.cap_node) {
+    if (!h->fixed_tree_cap && (4 * internal > 3 * h->t.cap_int || 4 * nodes > 3 * h->t.cap_node)) {
         int rc = alloc_tree(h, std::max<int64_t>(2 * internal + 1024, h->t.cap_int));
         if (rc) return rc;
         h->forces_valid = false;
@@ -710,17 +714,19 @@ int next_create(const next_params* p, next_handle** out) {
     auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
     A(&h->err, 1); A(&h->stats, 4); A(&h->queue, 1); A(&h->tickets, 4); A(&h->partial, kReduceMax * 8);
     A(&h->dts, 2); A(&h->dt_out, 2); A(&h->diag, 8); A(&h->changed, 4); A(&h->fma_out, 1);
-    A(&h->t.counts, 4);
+    A(&h->t.counts, 4); A(&h->done, 1);
     if (e != cudaSuccess) return bail(e, "scalars");
     e = cudaMemset(h->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->tickets, 0, sizeof(unsigned int) * 4);
     if (e == cudaSuccess) e = cudaMemset(h->stats, 0, sizeof(unsigned long long) * 4);
     if (e == cudaSuccess) e = cudaMemset(h->t.counts, 0, sizeof(int64_t) * 4);
+    if (e == cudaSuccess) e = cudaMemset(h->done, 0, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_dts), sizeof(double) * 2, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_err), sizeof(int) * 2, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_flags), sizeof(int) * 4, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_counts), sizeof(int64_t) * 4, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_stats), sizeof(unsigned long long) * 4, cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_done), sizeof(unsigned int), cudaHostAllocDefault);
     if (e != cudaSuccess) return bail(e, "pinned scalars");
     *out = h;
     return NEXT_OK;
@@ -736,6 +742,7 @@ void next_destroy(next_handle* h) {
     free_bodies(h);
     dfree(h->err); dfree(h->stats); dfree(h->queue); dfree(h->tickets); dfree(h->partial);
     dfree(h->dts); dfree(h->dt_out); dfree(h->diag); dfree(h->changed); dfree(h->fma_out); dfree(h->t.counts);
+    dfree(h->done);
     dfree(h->d_targets); dfree(h->d_targetpos); dfree(h->d_direct_partial); dfree(h->d_direct_out);
     if (h->flush) cudaFree(h->flush);
     for (auto ev : h->ev_pool) cudaEventDestroy(ev);
@@ -744,6 +751,7 @@ void next_destroy(next_handle* h) {
     if (h->h_flags) cudaFreeHost(h->h_flags);
     if (h->h_counts) cudaFreeHost(h->h_counts);
     if (h->h_stats) cudaFreeHost(h->h_stats);
+    if (h->h_done) cudaFreeHost(h->h_done);
     if (h->ev_out) cudaEventDestroy(h->ev_out);
     if (h->st_out) cudaStreamDestroy(h->st_out);
     if (h->st) cudaStreamDestroy(h->st);
@@ -964,21 +972,63 @@ int next_steps(next_handle* h, double dt, int nsteps) {
     rc = set_dt(h, dt);
     if (rc) return rc;
     const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces;
-    int done = 0;
+    int done = 0;            // steps completed
+    int base = 0;            // `done` when the device's count of completed replays was last zeroed
+    int since_check = 0;     // replays launched since the error word was last read
+    if (use_graph) NB_TRY(cudaMemsetAsync(h->done, 0, sizeof(unsigned int), h->st), "replay count");
+    // Reads the error word of the replays launched since the last look.  A
+    // replay that overflowed a capacity stopped after its kick-drift (every
+    // later kernel of it, and of the replays after it, skipped its work but
+    // the harmless body permutation), so the state is that step's drifted
+    // positions: grow what overflowed, redo its force phase and closing kick
+    // eagerly -- as step_once does -- and continue from the step after it.
+    auto check = [&]() -> int {
+        if (since_check == 0) return NEXT_OK;
+        since_check = 0;
+        NB_TRY(cudaMemcpyAsync(h->h_done, h->done, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->st),
+               "replay count");
+        int bits = 0;
+        int r = read_device_error(h, &bits);
+        if (r) return r;
+        if (bits == 0) return grow_if_tight(h);
+        const int completed = static_cast<int>(*h->h_done);
+        r = recover(h, bits);
+        if (r) return r;
+        r = forces_checked(h, false);
+        if (r) return r;
+        NB_TRY(launch_kick(h->cur_bodies(), h->n, h->dts, h->err, h->st), "kick");
+        h->forces_valid = true;
+        ++h->recoveries;
+        done = base + completed + 1;
+        base = done;
+        NB_TRY(cudaMemsetAsync(h->done, 0, sizeof(unsigned int), h->st), "replay count");
+        NB_TRY(cudaStreamSynchronize(h->st), "sync");
+        return NEXT_OK;
+    };
     while (done < nsteps) {
         if (!use_graph || !h->forces_valid) {
+            rc = check();
+            if (rc) return rc;
+            if (done >= nsteps) break;
             rc = step_once(h, !h->timing);
             if (rc) return rc;
             ++done;
+            base = done;
+            NB_TRY(cudaMemsetAsync(h->done, 0, sizeof(unsigned int), h->st), "replay count");
             continue;
         }
         // replay the captured step; buffers alternate, so keep one graph per parity
         if (!h->graph[h->cur]) {
-            int bits = 0;
-            rc = read_device_error(h, &bits);
+            rc = check();
             if (rc) return rc;
-            rc = grow_if_tight(h);
-            if (rc) return rc;
+            if (done >= nsteps) break;
+            if (since_check == 0) {
+                int bits = 0;
+                rc = read_device_error(h, &bits);
+                if (rc) return rc;
+                rc = grow_if_tight(h);
+                if (rc) return rc;
+            }
             if (!h->forces_valid) continue;
         }
         rc = capture_graph(h, true);
@@ -1004,16 +1054,14 @@ int next_steps(next_handle* h, double dt, int nsteps) {
         }
         h->cur = 1 - h->cur;
         ++done;
-        if (done == nsteps || (done & 63) == 0) {
-            int bits = 0;
-            rc = read_device_error(h, &bits);
-            if (rc) return rc;
-            if (bits) return fail(h, NEXT_ERR_DEVICE,
-                                  "device error word " + std::to_string(bits) + " during graph replay; use next_step");
-            rc = grow_if_tight(h);
+        ++since_check;
+        if (done == nsteps || since_check >= 64) {
+            rc = check();
             if (rc) return rc;
         }
     }
+    rc = check();
+    if (rc) return rc;
     h->forces_valid = true;
     return NEXT_OK;
 }
@@ -1118,6 +1166,7 @@ int next_stats_get(next_handle* h, next_stats* s) {
         s->n_nodes = h->h_counts[1];
         s->n_groups = h->h_counts[2];
         s->key_levels = h->sys.levels;
+        s->recoveries = static_cast<int32_t>(h->recoveries);
         s->pp_interactions = static_cast<int64_t>(h->h_stats[0]);
         s->pc_interactions = static_cast<int64_t>(h->h_stats[1]);
         s->max_stack = static_cast<int64_t>(h->h_stats[2]);
@@ -1391,6 +1440,34 @@ int next_autotune(next_handle* h, next_tune_result* out) {
         out->ms_force_phase = best_ms;
         out->candidates = tried;
     }
+    return NEXT_OK;
+}
+
+int next_debug_softening(int device, int64_t k, const double* size, const double* mass, const double* dist,
+                         double* out) {
+    if (k < 0 || (k > 0 && (!size || !mass || !dist || !out))) return NEXT_ERR_INVALID_ARGUMENT;
+    if (k == 0) return NEXT_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return NEXT_ERR_CUDA;
+    double* d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 4 * k) != cudaSuccess) return NEXT_ERR_OUT_OF_MEMORY;
+    cudaError_t e = cudaMemcpy(d, size, sizeof(double) * k, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + k, mass, sizeof(double) * k, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + 2 * k, dist, sizeof(double) * k, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_softening_eval(d, k, d + 3 * k, nullptr);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 3 * k, sizeof(double) * k, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? NEXT_OK : NEXT_ERR_CUDA;
+}
+
+int next_debug_fix_tree_capacity(next_handle* h, int64_t cap_internal) {
+    int rc = check_ready(h);
+    if (rc) return rc;
+    if (cap_internal < 1 || cap_internal >= (int64_t(1) << 31))
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "capacity out of range");
+    NB_TRY(cudaStreamSynchronize(h->st), "sync");
+    rc = alloc_tree(h, cap_internal);
+    if (rc) return rc;
+    h->fixed_tree_cap = true;     // the cached forces stay valid: they do not live in the tree
     return NEXT_OK;
 }
 

@@ -80,8 +80,14 @@ kick_drift_box_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const
     }
 }
 
-__global__ void kick_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err) {
+// The closing half-kick.  `done` (may be NULL) counts the kicks that ran:
+// a graph-replayed step only reaches it if nothing earlier in the step
+// raised an abort bit, so the count tells the host how many replayed steps
+// completed before one failed.
+__global__ void kick_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err,
+                            unsigned int* done) {
     if (*err & kErrAbort) return;
+    if (done && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(done, 1u);
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double half = dts[1];
@@ -278,9 +284,10 @@ cudaError_t launch_kick_drift_box(const Bodies& b, int64_t n, const double* dts,
     return cudaGetLastError();
 }
 
-cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st) {
+cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st,
+                        unsigned int* done) {
     if (n <= 0) return cudaSuccess;
-    kick_kernel<<<grid_for(n, 256), 256, 0, st>>>(b, n, dts, err);
+    kick_kernel<<<grid_for(n, 256), 256, 0, st>>>(b, n, dts, err, done);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -47,6 +47,8 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
 cudaError_t launch_walk_plain(const Bodies& bd, const int32_t* sysid, int64_t n, const Tree& t, const Params& P,
                               bool multi_system, unsigned long long* stats, int* err, cudaStream_t st);
 int direct_slices(int64_t n, int64_t k);
+// in: k sizes, k masses, k distances; out: k softening lengths (reference law)
+cudaError_t launch_softening_eval(const double* in, int64_t k, double* out, cudaStream_t st);
 cudaError_t launch_direct(const Bodies& bd, int64_t n, const int64_t* targets, int64_t k, double eps, double G,
                           double* partial, int slices, double* out, cudaStream_t st);
 
@@ -63,7 +65,8 @@ cudaError_t launch_kick_drift(const Bodies& b, int64_t n, const double* dts, con
 // kick-drift that also writes the root cube of the drifted bodies (one system)
 cudaError_t launch_kick_drift_box(const Bodies& b, int64_t n, const double* dts, const int* err, double* partial,
                                   int partial_blocks, unsigned int* ticket, double4* cube, cudaStream_t st);
-cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st);
+cudaError_t launch_kick(const Bodies& b, int64_t n, const double* dts, const int* err, cudaStream_t st,
+                        unsigned int* done = nullptr);
 int reduce_blocks(int64_t n);
 cudaError_t launch_adaptive_dt(const Bodies& b, int64_t n, double base_dt, double* partial, unsigned int* ticket,
                                double* out, cudaStream_t st);

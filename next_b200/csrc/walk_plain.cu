@@ -231,7 +231,20 @@ __global__ void direct_reduce_kernel(const double* __restrict__ partial, int64_t
     for (int c = 0; c < 4; ++c) out[4 * t + c] = s[c];
 }
 
+// The device softening law on k (size, mass, dist) triples (test support).
+__global__ void softening_kernel(const double* __restrict__ in, int64_t k, double* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t < k) out[t] = next_softening(in[t], in[k + t], in[2 * k + t]);
+}
+
 }  // namespace
+
+cudaError_t launch_softening_eval(const double* in, int64_t k, double* out, cudaStream_t st) {
+    if (k <= 0) return cudaSuccess;
+    softening_kernel<<<static_cast<unsigned>((k + 127) / 128), 128, 0, st>>>(in, k, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_walk_plain(const Bodies& bd, const int32_t* sysid, int64_t n, const Tree& t,
                               const Params& P, bool multi_system, unsigned long long* stats, int* err,

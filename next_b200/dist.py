@@ -9,6 +9,9 @@ own NCCL communicator on its own stream.
 Share of rank r: working positions [r*c, min(n, (r+1)*c)), c = ceil(n/world)
 -- the same formula the library uses, so every body has exactly one owner.
 Compare the reference's slice [r*N/size, (r+1)*N/size) (src/gravity/step.h:54-55).
+
+Independent systems (an ensemble) are not sliced by position but split
+whole over the ranks, balanced by their N log N work (split_systems).
 """
 from __future__ import annotations
 
@@ -28,6 +31,56 @@ def partition(n: int, world: int, rank: int):
     lo = min(n, rank * chunk)
     hi = min(n, lo + chunk)
     return lo, hi, chunk
+
+
+def padded_length(n: int, world: int) -> int:
+    """Length of each rank's force lanes: `world` equal chunks of ceil(n/world),
+    so the in-place all-gather sends chunk r from offset r*chunk of the same
+    buffer it receives into (the layout next_dist_attach allocates)."""
+    return -(-n // world) * world
+
+
+def system_cost(sizes):
+    """Work estimate of a Barnes-Hut step per system: N log2 N (walk
+    interactions grow as log N per body; the build is ~N per system)."""
+    import numpy as np
+    sizes = np.asarray(sizes, dtype=np.float64)
+    return sizes * np.log2(np.maximum(sizes, 2.0))
+
+
+def split_systems(sizes, world: int):
+    """Independent systems over `world` ranks, balanced by N log2 N.
+
+    Longest-processing-time greedy: systems in decreasing cost, each to the
+    rank with the least work so far (ties to the lower rank), which keeps the
+    largest rank load within a few per cent of the mean for ensembles of
+    uneven sizes.  Returns, per rank, the sorted system numbers it owns.
+    Every rank computes the same split from the same sizes.
+    """
+    import numpy as np
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    cost = system_cost(sizes)
+    order = np.lexsort((np.arange(cost.shape[0]), -cost))   # cost descending, stable by index
+    load = np.zeros(world)
+    owned = [[] for _ in range(world)]
+    for s in order:
+        r = int(np.argmin(load))
+        owned[r].append(int(s))
+        load[r] += cost[s]
+    return [np.array(sorted(o), dtype=np.int64) for o in owned]
+
+
+def select_systems(bodies, offsets, systems):
+    """The bodies of `systems` (sorted system numbers) and their new offsets."""
+    import numpy as np
+    offsets = np.asarray(offsets, dtype=np.int64)
+    idx = np.concatenate([np.arange(offsets[s], offsets[s + 1]) for s in systems]) if len(systems) else \
+        np.zeros(0, dtype=np.int64)
+    sizes = np.diff(offsets)[np.asarray(systems, dtype=np.int64)]
+    new_offsets = np.zeros(len(systems) + 1, dtype=np.int64)
+    new_offsets[1:] = np.cumsum(sizes)
+    return {k: v[idx] for k, v in bodies.items()}, new_offsets
 
 
 def broadcast_bytes(payload: bytes | None, size: int, src: int = 0, group=None) -> bytes:

@@ -36,7 +36,7 @@ class Stats(C.Structure):
                 ("pc_interactions", C.c_int64), ("max_stack", C.c_int64), ("device_error", C.c_int32),
                 ("steps", C.c_int32), ("ms_step", C.c_double), ("ms_build", C.c_double), ("ms_walk", C.c_double),
                 ("ms_sort", C.c_double), ("ms_other", C.c_double), ("walk_launches", C.c_int64),
-                ("key_levels", C.c_int32), ("reserved", C.c_int32)]
+                ("key_levels", C.c_int32), ("recoveries", C.c_int32)]
 
 
 # name -> (restype, argtypes)
@@ -69,6 +69,8 @@ SIGNATURES = {
     "next_debug_keys": (C.c_int, [_h, _u64, _d]),
     "next_debug_order": (C.c_int, [_h, _i64]),
     "next_debug_tree": (C.c_int, [_h, _d, C.c_int64, _i64]),
+    "next_debug_fix_tree_capacity": (C.c_int, [_h, C.c_int64]),
+    "next_debug_softening": (C.c_int, [C.c_int, C.c_int64, _d, _d, _d, _d]),
     "next_sort_pairs": (C.c_int, [_h, C.c_int64, _u64, _u32, _u64, _u32, C.c_int]),
     "next_fp32_peak": (C.c_int, [C.c_int, _d, _d]),
     "next_flush_l2": (C.c_int, [_h]),
@@ -123,6 +125,17 @@ def _p(a, t):
 
 def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def debug_softening(size, mass, dist, device: int = 0):
+    """The device's reference softening law on arrays of (size, mass, dist)."""
+    lib = load()
+    size, mass, dist = _f64(size), _f64(mass), _f64(dist)
+    out = np.empty(size.shape[0])
+    rc = lib.next_debug_softening(device, size.shape[0], _p(size, _d), _p(mass, _d), _p(dist, _d), _p(out, _d))
+    if rc:
+        raise NextError(f"next_debug_softening failed ({rc})")
+    return out
 
 
 def fp32_peak(device: int = 0) -> float:
@@ -299,6 +312,9 @@ class Simulation:
         self._check(self.lib.next_debug_tree(self.h, _p(rows, _d), cap, C.byref(nn)), "debug_tree")
         assert nn.value <= cap
         return rows[: nn.value]
+
+    def debug_fix_tree_capacity(self, cap_internal: int):
+        self._check(self.lib.next_debug_fix_tree_capacity(self.h, int(cap_internal)), "debug_fix_tree_capacity")
 
     def sort_pairs(self, keys, vals, key_bits: int = 64):
         keys = np.ascontiguousarray(keys, dtype=np.uint64)

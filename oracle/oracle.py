@@ -144,6 +144,7 @@ class Reference:
         L.ref_tree_export.argtypes = [C.c_int64, _d, _d, _d, _d, _d, C.c_int64]
         L.ref_tree_export.restype = C.c_int64
         L.ref_leaf_paths.argtypes = [C.c_int64, _d, _d, _d, _d, _u64, _i32]
+        L.ref_accel_sample.argtypes = [C.c_int64, _d, _d, _d, _d, _i32, C.c_double, C.c_int64, _i64, _d, _d, _d]
         L.ref_save_snapshot.argtypes = [C.c_int64, _d, _d, _d, _d, _d, _d, _d, _i32, C.c_int, C.c_char_p]
 
     def set_threads(self, k):
@@ -159,6 +160,18 @@ class Reference:
         ax, ay, az = np.zeros(n), np.zeros(n), np.zeros(n)
         self.lib.ref_accel(n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(t, _i32), theta,
                            _p(ax, _d), _p(ay, _d), _p(az, _d))
+        return {"ax": ax, "ay": ay, "az": az}
+
+    def accel_sample(self, b, idx, theta=0.5):
+        """bhAccel for the bodies idx only (one tree build, len(idx) walks)."""
+        n = b["x"].shape[0]
+        x, y, z, m = (_f64(b[k]) for k in ("x", "y", "z", "m"))
+        t = _i32a(b.get("type", np.zeros(n, np.int32)))
+        idx = np.ascontiguousarray(idx, dtype=np.int64)
+        k = idx.shape[0]
+        ax, ay, az = np.zeros(k), np.zeros(k), np.zeros(k)
+        self.lib.ref_accel_sample(n, _p(x, _d), _p(y, _d), _p(z, _d), _p(m, _d), _p(t, _i32), theta, k,
+                                  _p(idx, _i64), _p(ax, _d), _p(ay, _d), _p(az, _d))
         return {"ax": ax, "ay": ay, "az": az}
 
     def step(self, b, dt, nsteps=1):

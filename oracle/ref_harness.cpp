@@ -88,6 +88,23 @@ int ref_accel(int64_t n, const double* x, const double* y, const double* z,
     return 0;
 }
 
+// The same accelerations for the k bodies listed in idx only (one tree, k
+// walks): the reference's as-shipped force on a sample.
+int ref_accel_sample(int64_t n, const double* x, const double* y, const double* z,
+                     const double* m, const int* type, double theta, int64_t k, const int64_t* idx,
+                     double* ax, double* ay, double* az) {
+    if (n <= 0) return 0;
+    Particle ps = make_particles(n, x, y, z, nullptr, nullptr, nullptr, m, type);
+    auto root = build_reference_tree(ps);
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t t = 0; t < k; ++t) {
+        double a0 = 0, a1 = 0, a2 = 0;
+        bhAccel(root.get(), static_cast<int>(idx[t]), ps, theta, a0, a1, a2);
+        ax[t] = a0; ay[t] = a1; az[t] = a2;
+    }
+    return 0;
+}
+
 // nsteps calls of the reference's Step() (src/gravity/step.h:25), in place.
 int ref_step(int64_t n, double* x, double* y, double* z,
              double* vx, double* vy, double* vz,
