@@ -290,6 +290,36 @@ def plain_fp64_leg(bodies, offsets, cfg, device, steps, idx):
             "structure": "single-system plain FP64 step looped over 16 sampled systems (device time summed)"}
 
 
+def fp64_group_leg(bodies, offsets, cfg, device, steps, idx, d_direct, prm):
+    """The same algorithm in FP64: the group walk with the mixed run's tuned
+    leaf, group and block settings (so the same tree, groups and interaction
+    lists), force reuse and one graph replay per step -- only the precision of
+    the interactions differs from the headline step."""
+    from next_b200.native import Simulation
+    g = Simulation("accurate", "fp64group", theta=cfg["theta"], eps=cfg["eps"], device=device,
+                   leaf_cap=prm.leaf_cap, group_cap=prm.group_cap, walk_warps=prm.walk_warps,
+                   walk_stack=prm.walk_stack)
+    g.upload(bodies, offsets=offsets)
+    err = force_error(g.accel(), d_direct, idx) if d_direct is not None else None
+    g.steps(cfg["dt"], 2)
+    g.sync()
+    g.reset_timers()
+    g.set_timing(True)
+    for _ in range(steps):
+        g.flush_l2()
+        g.steps(cfg["dt"], 1)
+    g.sync()
+    st = g.stats()
+    g.close()
+    n = bodies["x"].shape[0]
+    flops = (FLOPS_PP * st["pp_interactions"] + FLOPS_PC * st["pc_interactions"]) / max(1, st["walk_launches"])
+    return {"value": n * steps / (st["ms_step"] * 1e-3), "unit": "particle-steps/s", "steps": steps,
+            "ms_per_step": st["ms_step"] / steps, "walk_ms": st["ms_walk"] / max(1, st["walk_launches"]),
+            "walk_tflops": flops / (st["ms_walk"] / max(1, st["walk_launches"]) * 1e-3) / 1e12,
+            "force_error": err,
+            "structure": "FP64 group walk: the mixed step's tree, groups, lists, force reuse and graph replay"}
+
+
 def ref_physics_leg(bodies, cfg, device, steps, idx, d_direct, cpu_accel):
     """The drop-in default: reference physics (adaptive softening, the
     reference's opening test and quadrupole) in plain FP64 on the GPU -- what
@@ -402,9 +432,12 @@ def run_ours(args):
     idx = np.random.default_rng(12345).choice(n, min(4096, n), replace=False)
     a_mixed = sim.accel()
     d_direct = None
+    state0 = None                           # the state d_direct belongs to: every leg's error is taken there
     if offsets is None:
         d_direct = sim.direct_accel(idx)
         err_mixed = force_error(a_mixed, d_direct, idx)
+        state0 = dict(bodies)
+        state0.update(sim.download())
     else:
         now = dict(bodies)
         now.update(sim.download())          # the direct sums must see the current positions
@@ -472,20 +505,20 @@ def run_ours(args):
     eager_ms = sim.stats()["ms_step"]
     sim.set_timing(False)
     fp64 = None
+    fp64g = None
     if rank == 0 and not args.skip_fp64:
         fp64 = plain_fp64_leg(bodies, offsets, W, local, max(1, args.fp64_steps), idx)
+        if world == 1:
+            fp64g = fp64_group_leg(state0 if state0 is not None else bodies, offsets, W, local,
+                                   max(3, args.steps // 4), idx, d_direct, sim.get_params())
     # the reference's as-shipped forces on the same sampled bodies, same state
     cpu_accel = None
-    now = None
-    if rank == 0 and offsets is None and d_direct is not None and not args.skip_cpu and n <= 2_000_000:
+    if rank == 0 and state0 is not None and not args.skip_cpu and n <= 2_000_000:
         from oracle.oracle import Reference
-        now = dict(bodies)
-        now.update(sim.download())
-        cpu_accel = Reference().accel_sample(now, idx)
+        cpu_accel = Reference().accel_sample(state0, idx)
     refphys = None
-    if rank == 0 and offsets is None and world == 1 and not args.skip_fp64:
-        refphys = ref_physics_leg(now if now is not None else bodies, W, local, max(1, args.fp64_steps), idx,
-                                  d_direct if now is not None else None, cpu_accel)
+    if rank == 0 and state0 is not None and world == 1 and not args.skip_fp64:
+        refphys = ref_physics_leg(state0, W, local, max(1, args.fp64_steps), idx, d_direct, cpu_accel)
     big_sort = None
     if rank == 0 and world == 1 and args.config == "c2" and not args.skip_large_sort:
         big_sort = large_sort_leg(W, local)
@@ -549,6 +582,8 @@ def run_ours(args):
                         "versus": "FP64 direct summation on seeded bodies"},
         "fp64_gpu": fp64,
         "speedup_vs_fp64_gpu": value / fp64["value"] if fp64 and world == 1 else None,
+        "fp64_same_structure_gpu": fp64g,
+        "speedup_vs_fp64_same_structure": value / fp64g["value"] if fp64g else None,
         "ref_physics_fp64_gpu": refphys,
         "eager_value": total_bodies * args.steps / (eager_ms * 1e-3) if eager_ms else None,
         "step_launch": "one CUDA-graph replay per KDK step (captured kick-drift + force phase + kick)",
@@ -572,7 +607,7 @@ def run_ours(args):
                               "walk": st["ms_walk"] / args.steps, "other": st["ms_other"] / args.steps},
         "energy_drift": abs(e1 - e0) / abs(e0),
         "autotune": tune,
-        "roofline": {"bound": "fp32", "kernel": "walk_mixed_kernel", "achieved": achieved, "peak": peak,
+        "roofline": {"bound": "fp32", "kernel": "walk_group_kernel<MixedArith<1,1,0>>", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "traffic": WALK_DRAM_BYTES if args.config == "c2" else None,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this workload",

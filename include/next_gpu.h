@@ -62,9 +62,14 @@ extern "C" {
  * NEXT_PRECISION_MIXED: FP32 interactions in a warp-per-group walk with
  *   shared-memory interaction lists and compensated accumulation; FP64 for
  *   positions, velocities, kick/drift, tree moments and diagnostics.
+ *   Requires NEXT_PHYSICS_ACCURATE.
+ * NEXT_PRECISION_FP64_GROUP: the same warp-per-group walk as MIXED -- same
+ *   leaf buckets, groups, interaction lists, force reuse and graph replays --
+ *   with every interaction in FP64.  It differs from MIXED in precision only.
  *   Requires NEXT_PHYSICS_ACCURATE. */
 #define NEXT_PRECISION_FP64 0
 #define NEXT_PRECISION_MIXED 1
+#define NEXT_PRECISION_FP64_GROUP 2
 
 typedef struct next_params {
     int physics;        /* NEXT_PHYSICS_* */
@@ -73,11 +78,11 @@ typedef struct next_params {
     double eps;         /* Plummer softening length (accurate mode) */
     double G;           /* gravitational constant (reference mode forces 1) */
     int leaf_cap;       /* bodies per leaf before a cell splits (reference mode forces 1) */
-    int group_cap;      /* bodies per walk group, <= 32 (mixed precision) */
+    int group_cap;      /* bodies per walk group, <= 32 (group walk: MIXED, FP64_GROUP) */
     int quadrupole;     /* 1: monopole + quadrupole; 0: monopole only (accurate mode) */
     int reuse_forces;   /* 1: the first half-kick reuses a(x_n) from the previous step */
-    int walk_warps;     /* warps per block of the mixed walk (1..4) */
-    int walk_stack;     /* per-warp traversal stack entries of the mixed walk */
+    int walk_warps;     /* warps per block of the group walk (1..4) */
+    int walk_stack;     /* per-warp traversal stack entries of the group walk */
     int device;         /* CUDA device ordinal */
 } next_params;
 

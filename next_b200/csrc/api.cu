@@ -354,12 +354,18 @@ int build(next_handle* h, std::vector<int>* evs) {
     return record(h, evs);
 }
 
+// The warp-per-group walk (FP32-mixed or FP64 arithmetic) with its leaf
+// buckets, trimmed keys, force reuse, graph replays and autotuner.
+bool group_walk(const next_handle* h) {
+    return h->prm.precision == NEXT_PRECISION_MIXED || h->prm.precision == NEXT_PRECISION_FP64_GROUP;
+}
+
 int walk(next_handle* h, bool potential) {
     Bodies bd = h->cur_bodies();
-    if (h->prm.precision == NEXT_PRECISION_MIXED) {
-        NB_TRY(launch_walk_mixed(bd, h->n, h->t, h->P, potential, h->prm.walk_warps, h->prm.walk_stack, h->queue, h->stats,
-                                 h->err, h->sm_count, h->st),
-               "mixed walk");
+    if (group_walk(h)) {
+        NB_TRY(launch_walk_group(bd, h->n, h->t, h->P, potential, h->prm.precision == NEXT_PRECISION_FP64_GROUP,
+                                 h->prm.walk_warps, h->prm.walk_stack, h->queue, h->stats, h->err, h->sm_count, h->st),
+               "group walk");
     } else {
         NB_TRY(launch_walk_plain(bd, h->sysid, h->n, h->t, h->P, h->nsys > 1, h->stats, h->err, h->st), "plain walk");
     }
@@ -405,7 +411,7 @@ void set_key_levels(next_handle* h, int levels) {
 }
 
 bool adaptive_depth(const next_handle* h) {
-    return h->prm.precision == NEXT_PRECISION_MIXED && h->P.physics == NEXT_PHYSICS_ACCURATE;
+    return group_walk(h) && h->P.physics == NEXT_PHYSICS_ACCURATE;
 }
 
 int read_device_error(next_handle* h, int* bits) {
@@ -631,7 +637,7 @@ int grow_if_tight(next_handle* h) {
         if (rc) return rc;
         h->forces_valid = false;
     }
-    if (h->prm.precision == NEXT_PRECISION_MIXED && 4 * static_cast<int64_t>(h->h_stats[2]) > 3 * h->prm.walk_stack &&
+    if (group_walk(h) && 4 * static_cast<int64_t>(h->h_stats[2]) > 3 * h->prm.walk_stack &&
         h->prm.walk_stack < (1 << 14)) {
         h->prm.walk_stack *= 2;
         drop_graphs(h);
@@ -666,10 +672,11 @@ int next_params_default(next_params* p, int physics, int precision) {
     p->theta = 0.5;
     p->eps = physics == NEXT_PHYSICS_REFERENCE ? 0.0 : 0.01;
     p->G = 1.0;
-    p->leaf_cap = physics == NEXT_PHYSICS_REFERENCE ? 1 : (precision == NEXT_PRECISION_MIXED ? 16 : 1);
+    const bool grouped = precision == NEXT_PRECISION_MIXED || precision == NEXT_PRECISION_FP64_GROUP;
+    p->leaf_cap = physics == NEXT_PHYSICS_REFERENCE ? 1 : (grouped ? 16 : 1);
     p->group_cap = 32;
     p->quadrupole = 1;
-    p->reuse_forces = precision == NEXT_PRECISION_MIXED ? 1 : 0;
+    p->reuse_forces = grouped ? 1 : 0;
     p->walk_warps = 4;
     p->walk_stack = 1024;
     p->device = 0;
@@ -679,13 +686,14 @@ int next_params_default(next_params* p, int physics, int precision) {
 int next_create(const next_params* p, next_handle** out) {
     if (!p || !out) return NEXT_ERR_INVALID_ARGUMENT;
     *out = nullptr;
+    const bool grouped = p->precision == NEXT_PRECISION_MIXED || p->precision == NEXT_PRECISION_FP64_GROUP;
     if ((p->physics != NEXT_PHYSICS_REFERENCE && p->physics != NEXT_PHYSICS_ACCURATE) ||
-        (p->precision != NEXT_PRECISION_FP64 && p->precision != NEXT_PRECISION_MIXED) ||
-        (p->precision == NEXT_PRECISION_MIXED && p->physics != NEXT_PHYSICS_ACCURATE) || !(p->theta > 0.0) ||
+        (p->precision != NEXT_PRECISION_FP64 && !grouped) ||
+        (grouped && p->physics != NEXT_PHYSICS_ACCURATE) || !(p->theta > 0.0) ||
         !(p->eps >= 0.0) || !std::isfinite(p->eps) || !std::isfinite(p->G) || p->leaf_cap < 1 || p->leaf_cap > 64 ||
         p->group_cap < 1 || p->group_cap > 32 || p->walk_warps < 1 || p->walk_warps > 4 || p->walk_stack < 64 ||
         p->walk_stack > (1 << 14) ||
-        (p->precision == NEXT_PRECISION_MIXED && p->leaf_cap > p->group_cap))
+        (grouped && p->leaf_cap > p->group_cap))
         return NEXT_ERR_INVALID_ARGUMENT;
     next_handle* h = new (std::nothrow) next_handle();
     if (!h) return NEXT_ERR_OUT_OF_MEMORY;
@@ -900,7 +908,7 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
     }
     // with mixed precision the force phase and the closing kick replay a
     // captured graph (one per buffer parity), as next_steps' steps do
-    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces;
+    const bool use_graph = group_walk(h) && h->prm.reuse_forces;
     if (use_graph && !h->fgraph[h->cur] && h->forces_valid) {
         rc = grow_if_tight(h);   // before a capture, as next_steps does
         if (rc) return rc;
@@ -971,7 +979,7 @@ int next_steps(next_handle* h, double dt, int nsteps) {
     if (!std::isfinite(dt) || nsteps < 0) return fail(h, NEXT_ERR_INVALID_ARGUMENT, "bad dt or step count");
     rc = set_dt(h, dt);
     if (rc) return rc;
-    const bool use_graph = h->prm.precision == NEXT_PRECISION_MIXED && h->prm.reuse_forces;
+    const bool use_graph = group_walk(h) && h->prm.reuse_forces;
     int done = 0;            // steps completed
     int base = 0;            // `done` when the device's count of completed replays was last zeroed
     int since_check = 0;     // replays launched since the error word was last read
@@ -1358,8 +1366,8 @@ int64_t next_kernel_launches(void) { return launches_so_far(); }
 int next_autotune(next_handle* h, next_tune_result* out) {
     int rc = check_ready(h);
     if (rc) return rc;
-    if (h->prm.precision != NEXT_PRECISION_MIXED)
-        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "autotuning applies to the mixed-precision walk");
+    if (!group_walk(h))
+        return fail(h, NEXT_ERR_INVALID_ARGUMENT, "autotuning applies to the group walk (mixed or FP64-group precision)");
     struct Cand { int leaf, group, warps; };
     std::vector<Cand> cands;
     for (int g : {16, 24, 32})

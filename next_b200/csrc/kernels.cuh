@@ -52,11 +52,11 @@ cudaError_t launch_softening_eval(const double* in, int64_t k, double* out, cuda
 cudaError_t launch_direct(const Bodies& bd, int64_t n, const int64_t* targets, int64_t k, double eps, double G,
                           double* partial, int slices, double* out, cudaStream_t st);
 
-// walk_mixed.cu
-size_t walk_mixed_smem(int warps, int stack_cap);
-cudaError_t launch_walk_mixed(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, bool potential, int warps,
-                              int stack_cap, unsigned int* queue, unsigned long long* stats, int* err, int sm_count,
-                              cudaStream_t st);
+// walk_group.cu: the warp-per-group walk, FP32-mixed or FP64 arithmetic
+size_t walk_group_smem(bool fp64, int warps, int stack_cap);
+cudaError_t launch_walk_group(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, bool potential,
+                              bool fp64, int warps, int stack_cap, unsigned int* queue, unsigned long long* stats,
+                              int* err, int sm_count, cudaStream_t st);
 
 // integrate.cu
 cudaError_t launch_gather_bodies(const Bodies& src, const Bodies& dst, const uint32_t* idx, int64_t n, uint32_t* inv,

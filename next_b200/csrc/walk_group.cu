@@ -1,5 +1,10 @@
-// Mixed-precision force walk: one warp per group of <= 32 Morton-contiguous
-// target bodies, FP32 interactions, compensated accumulation.
+// Group force walk: one warp per group of <= 32 Morton-contiguous target
+// bodies, in two arithmetics over the same traversal:
+//   * FP32-mixed (NEXT_PRECISION_MIXED): FP32 interactions, compensated
+//     accumulation;
+//   * FP64 (NEXT_PRECISION_FP64_GROUP): the same interaction lists -- same
+//     tree, groups and opening decisions -- evaluated in FP64, so the two
+//     differ in precision only.
 //
 // Traversal: a per-warp LIFO stack of node ids in shared memory; each round
 // pops up to 32 nodes (one per lane) and applies the opening test
@@ -13,14 +18,16 @@
 // rounded to FP32 -- coordinates relative to the group keep FP32 exact
 // enough near the group) and every lane runs the 32 interactions for its
 // target from shared memory with FP32 FMA and rsqrt.  The 32-term partial
-// is folded into the per-target sum with Kahan compensation.
+// is folded into the per-target sum with Kahan compensation.  The FP64
+// arithmetic stages the same entries in FP64 and sums them in FP64.
 //
 // Scheduling: persistent blocks (SM count x resident blocks) pull groups
 // from a global atomic work queue.  All waits are warp-synchronous; there
 // are no inter-block waits.  Stack or list overflow raises an error bit and
 // abandons the group.
 //
-// Roofline: FP32 pipe.  Algorithmic flops: 20 per PP, 56 per PC interaction.
+// Roofline: FP32 pipe (FP64 pipe for the FP64 arithmetic).  Algorithmic
+// flops: 20 per PP, 56 per PC interaction.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -45,6 +52,9 @@ namespace {
 #ifndef NB_WALK_MIN_BLOCKS
 #define NB_WALK_MIN_BLOCKS 6
 #endif
+#ifndef NB_WALK64_MIN_BLOCKS
+#define NB_WALK64_MIN_BLOCKS 4
+#endif
 
 constexpr int kWalkUnroll = NB_WALK_UNROLL;
 constexpr int kWalkGenericUnroll = NB_WALK_GENERIC_UNROLL;
@@ -52,8 +62,10 @@ constexpr int kPcCap = 64;
 constexpr int kPpChunk = 16;
 constexpr int kPpCap = 32 + 32 * kPpChunk;
 
-struct WarpLists {
-    float4 stage[3 * 32];
+// Per-warp shared lists; STAGE_BYTES hold one staged evaluation batch.
+template <int STAGE_BYTES>
+struct WarpListsT {
+    alignas(16) unsigned char stage[STAGE_BYTES];
     double gc[4];                // FP64 group centre, read back at each staging
     int pc[kPcCap];
     int pp[kPpCap];
@@ -347,60 +359,201 @@ __device__ __forceinline__ void stage_pp_packed(float4* stage, const int* list, 
 // Stage up to 32 cells (one per lane) and evaluate them.  PACK stages them in
 // pairs for the .f32x2 path (lanes past `count` stage zero-mass entries).
 template <bool QUAD, bool POT, bool PACK>
-__device__ __forceinline__ void eval_pc(WarpLists& L, const int* list, int count, const Tree& t, double gcx,
+__device__ __forceinline__ void eval_pc(float4* stage, const int* list, int count, const Tree& t, double gcx,
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
     if (PACK) {
-        stage_pc_packed<QUAD>(L.stage, list, count, t, gcx, gcy, gcz, G, lane);
+        stage_pc_packed<QUAD>(stage, list, count, t, gcx, gcy, gcz, G, lane);
         __syncwarp();
-        eval_batch_packed<5, true, QUAD>(L.stage, count, eps2, active, slice, nslices, T);
+        eval_batch_packed<5, true, QUAD>(stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
         return;
     }
     if (lane < count) {
         const int node = list[lane];
         const double4 c = t.com[node];
-        L.stage[3 * lane + 0] = make_float4(static_cast<float>(c.x - gcx), static_cast<float>(c.y - gcy),
-                                            static_cast<float>(c.z - gcz), static_cast<float>(G * c.w));
+        stage[3 * lane + 0] = make_float4(static_cast<float>(c.x - gcx), static_cast<float>(c.y - gcy),
+                                          static_cast<float>(c.z - gcz), static_cast<float>(G * c.w));
         if (QUAD) {
-            L.stage[3 * lane + 1] = t.quad32[2 * node];
-            L.stage[3 * lane + 2] = t.quad32[2 * node + 1];
+            stage[3 * lane + 1] = t.quad32[2 * node];
+            stage[3 * lane + 2] = t.quad32[2 * node + 1];
         }
     }
     __syncwarp();
-    eval_batch<3, true, QUAD, POT>(L.stage, count, eps2, active, slice, nslices, T);
+    eval_batch<3, true, QUAD, POT>(stage, count, eps2, active, slice, nslices, T);
     __syncwarp();
 }
 
 // Stage up to 32 bodies (one per lane) and evaluate them.
 template <bool SOFT, bool POT, bool PACK>
-__device__ __forceinline__ void eval_pp(WarpLists& L, const int* list, int count, const Bodies& bd, double gcx,
+__device__ __forceinline__ void eval_pp(float4* stage, const int* list, int count, const Bodies& bd, double gcx,
                                         double gcy, double gcz, float G, float eps2, bool active, int slice,
                                         int nslices, Target& T, int lane) {
     if (PACK) {
-        stage_pp_packed(L.stage, list, count, bd, gcx, gcy, gcz, G, lane);
+        stage_pp_packed(stage, list, count, bd, gcx, gcy, gcz, G, lane);
         __syncwarp();
-        eval_batch_packed<2, false, false>(L.stage, count, eps2, active, slice, nslices, T);
+        eval_batch_packed<2, false, false>(stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
         return;
     }
     if (lane < count) {
         const int j = list[lane];
-        L.stage[lane] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
-                                    static_cast<float>(bd.z[j] - gcz), static_cast<float>(G * bd.m[j]));
+        stage[lane] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
+                                  static_cast<float>(bd.z[j] - gcz), static_cast<float>(G * bd.m[j]));
     }
     __syncwarp();
-    eval_batch<1, false, SOFT, POT>(L.stage, count, eps2, active, slice, nslices, T);
+    eval_batch<1, false, SOFT, POT>(stage, count, eps2, active, slice, nslices, T);
     __syncwarp();
 }
 
+// ---- the two arithmetics of the walk -----------------------------------------
+// Each provides the staging buffer size, the per-lane accumulator, the
+// evaluation of a PC and a PP batch, and the final FP64 sums.
+
 template <bool QUAD, bool SOFT, bool POT>
-__global__ void __launch_bounds__(128, NB_WALK_MIN_BLOCKS)
-walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int stack_cap, unsigned int* queue,
-                  unsigned long long* stats, int* err, int64_t own_lo, int64_t own_hi) {
-    if (*err & kErrAbort) return;
+struct MixedArith {
+    using Scalar = float;
     // softened forces without the potential take the packed two-entry path
-    constexpr bool kPack = NB_WALK_PACKED && SOFT && !POT;
+    static constexpr bool kPack = NB_WALK_PACKED && SOFT && !POT;
+    static constexpr int kStageBytes = 3 * 32 * sizeof(float4);
+    static constexpr int kMinBlocks = NB_WALK_MIN_BLOCKS;
+    static constexpr bool kPot = POT;
+    using Acc = Target;
+    __device__ static void start(Acc& T, double px, double py, double pz, double gcx, double gcy, double gcz) {
+        T.tx = static_cast<float>(px - gcx); T.ty = static_cast<float>(py - gcy); T.tz = static_cast<float>(pz - gcz);
+        T.ax = T.ay = T.az = T.pot = 0.f;
+        T.cx = T.cy = T.cz = T.cp = 0.f;
+    }
+    __device__ static void pc(unsigned char* stage, const int* list, int count, const Tree& t, const Bodies&,
+                              double gcx, double gcy, double gcz, float G, float eps2, bool active, int slice,
+                              int nslices, Acc& T, int lane) {
+        eval_pc<QUAD, POT, kPack>(reinterpret_cast<float4*>(stage), list, count, t, gcx, gcy, gcz, G, eps2, active,
+                                  slice, nslices, T, lane);
+    }
+    __device__ static void pp(unsigned char* stage, const int* list, int count, const Tree&, const Bodies& bd,
+                              double gcx, double gcy, double gcz, float G, float eps2, bool active, int slice,
+                              int nslices, Acc& T, int lane) {
+        eval_pp<SOFT, POT, kPack>(reinterpret_cast<float4*>(stage), list, count, bd, gcx, gcy, gcz, G, eps2, active,
+                                  slice, nslices, T, lane);
+    }
+    __device__ static void finish(const Acc& T, double& fx, double& fy, double& fz, double& fp) {
+        fx = static_cast<double>(T.ax) - static_cast<double>(T.cx);
+        fy = static_cast<double>(T.ay) - static_cast<double>(T.cy);
+        fz = static_cast<double>(T.az) - static_cast<double>(T.cz);
+        fp = POT ? static_cast<double>(T.pot) - static_cast<double>(T.cp) : 0.0;
+    }
+};
+
+// FP64: entries staged as 10 (PC) or 4 (PP) doubles relative to the group
+// centre, -G Q for the quadrupole; FP64 FMA and rsqrt, FP64 sums.
+template <bool QUAD, bool SOFT, bool POT>
+struct Fp64Arith {
+    using Scalar = double;
+    static constexpr int kStageBytes = 32 * 10 * sizeof(double);
+    static constexpr int kMinBlocks = NB_WALK64_MIN_BLOCKS;
+    static constexpr bool kPot = POT;
+    struct Acc {
+        double tx, ty, tz, ax, ay, az, pot;
+    };
+    __device__ static void start(Acc& A, double px, double py, double pz, double gcx, double gcy, double gcz) {
+        A.tx = px - gcx; A.ty = py - gcy; A.tz = pz - gcz;
+        A.ax = A.ay = A.az = A.pot = 0.0;
+    }
+    // one body-cell term: a = rinv3 (G m - 2.5 q rinv4) d + rinv5 qd with the
+    // negated Q staged (qd = -G Q d, q = -G d.Q.d), as the FP32 pc_term
+    __device__ static void pc_term(const double* e, Acc& A, double eps2) {
+        const double dx = e[0] - A.tx, dy = e[1] - A.ty, dz = e[2] - A.tz, m = e[3];
+        const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+        const double rinv = rsqrt(r2);
+        const double rinv2 = rinv * rinv;
+        const double rinv3 = rinv2 * rinv;
+        if (QUAD) {
+            const double qdx = fma(e[8], dz, fma(e[7], dy, e[4] * dx));
+            const double qdy = fma(e[9], dz, fma(e[5], dy, e[7] * dx));
+            const double qdz = fma(e[6], dz, fma(e[9], dy, e[8] * dx));
+            const double q = fma(dz, qdz, fma(dy, qdy, dx * qdx));
+            const double cc = rinv3 * fma(q, (-2.5 * rinv2) * rinv2, m);
+            const double rinv5 = rinv3 * rinv2;
+            A.ax = fma(cc, dx, fma(rinv5, qdx, A.ax));
+            A.ay = fma(cc, dy, fma(rinv5, qdy, A.ay));
+            A.az = fma(cc, dz, fma(rinv5, qdz, A.az));
+            if (POT) A.pot = fma(0.5 * q, rinv5, fma(-m, rinv, A.pot));
+        } else {
+            const double mr3 = m * rinv3;
+            A.ax = fma(mr3, dx, A.ax);
+            A.ay = fma(mr3, dy, A.ay);
+            A.az = fma(mr3, dz, A.az);
+            if (POT) A.pot = fma(-m, rinv, A.pot);
+        }
+    }
+    __device__ static void pp_term(const double* e, Acc& A, double eps2) {
+        const double dx = e[0] - A.tx, dy = e[1] - A.ty, dz = e[2] - A.tz;
+        const double r2 = fma(dz, dz, fma(dy, dy, fma(dx, dx, eps2)));
+        double rinv = rsqrt(r2);
+        if (!SOFT) rinv = r2 > 0.0 ? rinv : 0.0;     // the target itself, unsoftened
+        const double mr = e[3] * rinv;
+        const double mr3 = mr * rinv * rinv;
+        A.ax = fma(mr3, dx, A.ax);
+        A.ay = fma(mr3, dy, A.ay);
+        A.az = fma(mr3, dz, A.az);
+        if (POT) A.pot -= r2 > eps2 ? mr : 0.0;        // no self term
+    }
+    template <int STRIDE, bool PC>
+    __device__ static void run(const double* st, int count, double eps2, bool active, int slice, int nslices,
+                               Acc& A) {
+        if (!active) return;
+        const int chunk = (count + nslices - 1) / nslices;
+        const int k0 = slice * chunk;
+        const int k1 = min(count, k0 + chunk);
+#pragma unroll 4
+        for (int k = k0; k < k1; ++k) {
+            if (PC) pc_term(st + STRIDE * k, A, eps2);
+            else pp_term(st + STRIDE * k, A, eps2);
+        }
+    }
+    __device__ static void pc(unsigned char* stage, const int* list, int count, const Tree& t, const Bodies&,
+                              double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
+                              int nslices, Acc& A, int lane) {
+        double* st = reinterpret_cast<double*>(stage);
+        if (lane < count) {
+            const int node = list[lane];
+            const double4 c = t.com[node];
+            double* e = st + 10 * lane;
+            e[0] = c.x - gcx; e[1] = c.y - gcy; e[2] = c.z - gcz; e[3] = G * c.w;
+            if (QUAD) {
+                const double* q = t.quad64 + 8 * static_cast<int64_t>(node);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) e[4 + k] = -G * q[k];
+            }
+        }
+        __syncwarp();
+        run<10, true>(st, count, eps2, active, slice, nslices, A);
+        __syncwarp();
+    }
+    __device__ static void pp(unsigned char* stage, const int* list, int count, const Tree&, const Bodies& bd,
+                              double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
+                              int nslices, Acc& A, int lane) {
+        double* st = reinterpret_cast<double*>(stage);
+        if (lane < count) {
+            const int j = list[lane];
+            double* e = st + 4 * lane;
+            e[0] = bd.x[j] - gcx; e[1] = bd.y[j] - gcy; e[2] = bd.z[j] - gcz; e[3] = G * bd.m[j];
+        }
+        __syncwarp();
+        run<4, false>(st, count, eps2, active, slice, nslices, A);
+        __syncwarp();
+    }
+    __device__ static void finish(const Acc& A, double& fx, double& fy, double& fz, double& fp) {
+        fx = A.ax; fy = A.ay; fz = A.az; fp = POT ? A.pot : 0.0;
+    }
+};
+
+template <class A>
+__global__ void __launch_bounds__(128, A::kMinBlocks)
+walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, typename A::Scalar eps2, int stack_cap,
+                  unsigned int* queue, unsigned long long* stats, int* err, int64_t own_lo, int64_t own_hi) {
+    if (*err & kErrAbort) return;
+    using WarpLists = WarpListsT<A::kStageBytes>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
@@ -454,10 +607,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
         const float hx = static_cast<float>(0.5 * (hix - lox)) * 1.000001f + pad;
         const float hy = static_cast<float>(0.5 * (hiy - loy)) * 1.000001f + pad;
         const float hz = static_cast<float>(0.5 * (hiz - loz)) * 1.000001f + pad;
-        Target T;
-        T.tx = static_cast<float>(px - gcx); T.ty = static_cast<float>(py - gcy); T.tz = static_cast<float>(pz - gcz);
-        T.ax = T.ay = T.az = T.pot = 0.f;
-        T.cx = T.cy = T.cz = T.cp = 0.f;
+        typename A::Acc T;
+        A::start(T, px, py, pz, gcx, gcy, gcz);
 
         int sp = 1, pc_n = 0, pp_n = 0;
         if (lane == 0) stack[0] = grp.z;
@@ -504,7 +655,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
             if (pc_n >= 32) {
-                eval_pc<QUAD, POT, kPack>(L, L.pc, 32, t, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane);
+                A::pc(L.stage, L.pc, 32, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
+                      nslices, T, lane);
                 g_pc += 32;
                 pc_n -= 32;
                 const int v = lane < pc_n ? L.pc[32 + lane] : 0;
@@ -525,7 +677,8 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
                 __syncwarp();
                 int head = 0;
                 while (pp_n - head >= 32) {
-                    eval_pp<SOFT, POT, kPack>(L, L.pp + head, 32, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane);
+                    A::pp(L.stage, L.pp + head, 32, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active,
+                          slice, nslices, T, lane);
                     g_pp += 32;
                     head += 32;
                 }
@@ -542,23 +695,29 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
             if (lane == 0) raise_error(err, kErrStack);
             continue;
         }
-        if (pc_n > 0) { eval_pc<QUAD, POT, kPack>(L, L.pc, pc_n, t, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane); g_pc += pc_n; }
-        if (pp_n > 0) { eval_pp<SOFT, POT, kPack>(L, L.pp, pp_n, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice, nslices, T, lane); g_pp += pp_n; }
-        double fx = static_cast<double>(T.ax) - static_cast<double>(T.cx);
-        double fy = static_cast<double>(T.ay) - static_cast<double>(T.cy);
-        double fz = static_cast<double>(T.az) - static_cast<double>(T.cz);
-        double fp = POT ? static_cast<double>(T.pot) - static_cast<double>(T.cp) : 0.0;
+        if (pc_n > 0) {
+            A::pc(L.stage, L.pc, pc_n, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
+                  nslices, T, lane);
+            g_pc += pc_n;
+        }
+        if (pp_n > 0) {
+            A::pp(L.stage, L.pp, pp_n, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
+                  nslices, T, lane);
+            g_pp += pp_n;
+        }
+        double fx, fy, fz, fp;
+        A::finish(T, fx, fy, fz, fp);
         for (int o = width; o < 32; o <<= 1) {
             fx += __shfl_xor_sync(0xffffffffu, fx, o);
             fy += __shfl_xor_sync(0xffffffffu, fy, o);
             fz += __shfl_xor_sync(0xffffffffu, fz, o);
-            if (POT) fp += __shfl_xor_sync(0xffffffffu, fp, o);
+            if (A::kPot) fp += __shfl_xor_sync(0xffffffffu, fp, o);
         }
         if (active && slice == 0 && i >= own_lo && i < own_hi) {
             bd.ax[i] = fx;
             bd.ay[i] = fy;
             bd.az[i] = fz;
-            if (POT && bd.pot) bd.pot[i] = fp;
+            if (A::kPot && bd.pot) bd.pot[i] = fp;
         }
         npp += static_cast<unsigned long long>(g_pp) * own_nt;
         npc += static_cast<unsigned long long>(g_pc) * own_nt;
@@ -570,12 +729,12 @@ walk_mixed_kernel(Bodies bd, int64_t nbodies, Tree t, float G, float eps2, int s
     }
 }
 
-template <bool QUAD, bool SOFT, bool POT>
+template <class A>
 cudaError_t launch_variant(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, int warps, int stack_cap,
                            unsigned int* queue, unsigned long long* stats, int* err, int sm_count,
                            cudaStream_t st) {
-    auto kern = walk_mixed_kernel<QUAD, SOFT, POT>;
-    const size_t smem = (sizeof(WarpLists) + sizeof(int) * stack_cap) * warps;
+    auto kern = walk_group_kernel<A>;
+    const size_t smem = (sizeof(WarpListsT<A::kStageBytes>) + sizeof(int) * stack_cap) * warps;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
@@ -584,31 +743,48 @@ cudaError_t launch_variant(const Bodies& bd, int64_t nbodies, const Tree& t, con
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     e = cudaMemsetAsync(queue, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
-    kern<<<per_sm * sm_count, 32 * warps, smem, st>>>(bd, nbodies, t, static_cast<float>(P.G),
-                                                     static_cast<float>(P.eps * P.eps), stack_cap, queue, stats, err,
+    using S = typename A::Scalar;
+    kern<<<per_sm * sm_count, 32 * warps, smem, st>>>(bd, nbodies, t, static_cast<S>(P.G),
+                                                     static_cast<S>(P.eps * P.eps), stack_cap, queue, stats, err,
                                                      P.own_lo, P.own_hi);
     count_launches(1);
     return cudaGetLastError();
 }
 
+template <template <bool, bool, bool> class Arith>
+cudaError_t launch_arith(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, bool potential, int warps,
+                         int stack_cap, unsigned int* queue, unsigned long long* stats, int* err, int sm_count,
+                         cudaStream_t st) {
+    const bool soft = P.eps > 0.0;
+#define NB_WALK_CASE(Q, S, POT)                                                                                  \
+    if (P.quad == Q && soft == S && potential == POT)                                                            \
+        return launch_variant<Arith<Q, S, POT>>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st);
+    NB_WALK_CASE(true, true, false)
+    NB_WALK_CASE(true, true, true)
+    NB_WALK_CASE(true, false, false)
+    NB_WALK_CASE(true, false, true)
+    NB_WALK_CASE(false, true, false)
+    NB_WALK_CASE(false, true, true)
+    NB_WALK_CASE(false, false, false)
+    NB_WALK_CASE(false, false, true)
+#undef NB_WALK_CASE
+    return cudaErrorInvalidValue;
+}
+
 }  // namespace
 
-size_t walk_mixed_smem(int warps, int stack_cap) { return (sizeof(WarpLists) + sizeof(int) * stack_cap) * warps; }
+size_t walk_group_smem(bool fp64, int warps, int stack_cap) {
+    const size_t lists = fp64 ? sizeof(WarpListsT<Fp64Arith<true, true, false>::kStageBytes>)
+                              : sizeof(WarpListsT<MixedArith<true, true, false>::kStageBytes>);
+    return (lists + sizeof(int) * stack_cap) * warps;
+}
 
-cudaError_t launch_walk_mixed(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, bool potential, int warps,
-                              int stack_cap, unsigned int* queue, unsigned long long* stats, int* err,
-                              int sm_count, cudaStream_t st) {
-    const bool soft = P.eps > 0.0;
-    if (P.quad) {
-        if (soft) return potential ? launch_variant<true, true, true>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st)
-                                   : launch_variant<true, true, false>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st);
-        return potential ? launch_variant<true, false, true>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st)
-                         : launch_variant<true, false, false>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st);
-    }
-    if (soft) return potential ? launch_variant<false, true, true>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st)
-                               : launch_variant<false, true, false>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st);
-    return potential ? launch_variant<false, false, true>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st)
-                     : launch_variant<false, false, false>(bd, nbodies, t, P, warps, stack_cap, queue, stats, err, sm_count, st);
+cudaError_t launch_walk_group(const Bodies& bd, int64_t nbodies, const Tree& t, const Params& P, bool potential,
+                              bool fp64, int warps, int stack_cap, unsigned int* queue, unsigned long long* stats,
+                              int* err, int sm_count, cudaStream_t st) {
+    if (fp64)
+        return launch_arith<Fp64Arith>(bd, nbodies, t, P, potential, warps, stack_cap, queue, stats, err, sm_count, st);
+    return launch_arith<MixedArith>(bd, nbodies, t, P, potential, warps, stack_cap, queue, stats, err, sm_count, st);
 }
 
 }  // namespace nb

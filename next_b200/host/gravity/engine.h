@@ -4,7 +4,7 @@
 // Configuration comes from next_gpu::configure() or, when that was not
 // called, from the environment:
 //   NEXT_PHYSICS   reference (default) | accurate
-//   NEXT_PRECISION fp64 (default)      | mixed     (mixed needs accurate)
+//   NEXT_PRECISION fp64 (default)      | mixed | fp64group   (the last two need accurate)
 //   NEXT_THETA, NEXT_EPS, NEXT_LEAF_CAP, NEXT_DEVICE
 // The default reproduces the reference's physics (theta 0.5 on half-widths,
 // adaptive softening, its quadrupole) with FP64 arithmetic on the GPU.
@@ -25,7 +25,8 @@ inline next_params params_from_env() {
     const std::string prec = get("NEXT_PRECISION") ? get("NEXT_PRECISION") : "fp64";
     next_params p;
     next_params_default(&p, phys == "accurate" ? NEXT_PHYSICS_ACCURATE : NEXT_PHYSICS_REFERENCE,
-                        prec == "mixed" ? NEXT_PRECISION_MIXED : NEXT_PRECISION_FP64);
+                        prec == "mixed" ? NEXT_PRECISION_MIXED
+                                        : prec == "fp64group" ? NEXT_PRECISION_FP64_GROUP : NEXT_PRECISION_FP64);
     if (get("NEXT_THETA")) p.theta = std::atof(get("NEXT_THETA"));
     if (get("NEXT_EPS")) p.eps = std::atof(get("NEXT_EPS"));
     if (get("NEXT_LEAF_CAP")) p.leaf_cap = std::atoi(get("NEXT_LEAF_CAP"));

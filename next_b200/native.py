@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("NEXT_B200_LIB") or os.path.join(HERE, "lib", "libnext_b200.so")
 
 PHYSICS = {"reference": 0, "accurate": 1}
-PRECISION = {"fp64": 0, "mixed": 1}
+PRECISION = {"fp64": 0, "mixed": 1, "fp64group": 2}
 DEVERR = {1: "tree capacity", 2: "walk stack", 4: "sort look-back timeout", 8: "interaction list"}
 
 

@@ -232,6 +232,63 @@ def test_mixed_precision_force_error(oracle, maker, n, theta, eps):
     sim.close()
 
 
+@pytest.mark.parametrize("maker,n,theta,eps", [
+    (ic.plummer, 16_384, 0.5, 0.01),
+    (ic.hernquist, 65_536, 0.7, 0.002),
+])
+def test_fp64_group_walk_is_the_mixed_walk_in_fp64(oracle, maker, n, theta, eps):
+    """NEXT_PRECISION_FP64_GROUP walks exactly the interaction lists of the
+    FP32-mixed walk (same PP and PC counts) in FP64: the two differ by FP32
+    rounding only, and both meet the bar against FP64 direct summation."""
+    b = maker(n)
+    g = Simulation("accurate", "fp64group", theta=theta, eps=eps)
+    x = Simulation("accurate", "mixed", theta=theta, eps=eps)
+    g.upload(b)
+    x.upload(b)
+    ag, ax_ = g.accel(), x.accel()
+    sg, sx = g.stats(), x.stats()
+    assert sg["pp_interactions"] == sx["pp_interactions"] and sg["pc_interactions"] == sx["pc_interactions"]
+    assert float(np.median(rel_err(ax_, ag))) <= 2e-6
+    idx = np.random.default_rng(0).choice(n, 1024, replace=False)
+    d = oracle.direct(b, idx, eps=eps)
+    eg = rel_err({c: ag[c][idx] for c in ag}, d)
+    assert np.median(eg) <= 1e-3 and np.percentile(eg, 99) <= 1e-2
+    g.close()
+    x.close()
+
+
+def test_fp64_group_walk_opening_everything_is_direct_summation(oracle):
+    """With theta -> 0 every cell is opened, so the FP64 group walk is a direct
+    sum over all bodies in FP64: relative 1e-12 against the oracle, potential
+    included."""
+    b = ic.plummer(4096, seed=17)
+    g = Simulation("accurate", "fp64group", theta=1e-4, eps=0.01)
+    g.upload(b)
+    a = g.accel(potential=True)
+    d = oracle.direct(b, np.arange(4096), eps=0.01)
+    assert float(np.max(rel_err(a, d))) <= 1e-12
+    assert float(np.max(np.abs(a["pot"] - d["pot"]) / np.abs(d["pot"]))) <= 1e-12
+    st = g.stats()
+    assert st["pc_interactions"] == 0 and st["pp_interactions"] == 4096 * 4096
+    g.close()
+
+
+def test_fp64_group_graph_steps_equal_eager_steps():
+    b = ic.plummer(20_000, seed=8)
+    a = Simulation("accurate", "fp64group")
+    g = Simulation("accurate", "fp64group")
+    a.upload(b)
+    g.upload(b)
+    for _ in range(5):
+        a.step(1e-3)
+    g.steps(1e-3, 5)
+    sa, sg = a.download(), g.download()
+    for c in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(sa[c], sg[c])
+    a.close()
+    g.close()
+
+
 def test_mixed_steps_trim_key_depth(oracle):
     """After the first build the FP32-mixed path keeps only the measured tree
     depth + 3 octant levels in its keys; forces stay as accurate and match a
@@ -503,7 +560,7 @@ def test_reuse_forces_matches_recompute():
 
 def test_ensemble_equals_independent_systems():
     bodies, offs = ic.ensemble(n_systems=8, seed=3, nmin=500, nmax=5000)
-    for precision, leaf in (("fp64", 1), ("mixed", 16)):
+    for precision, leaf in (("fp64", 1), ("mixed", 16), ("fp64group", 16)):
         ens = Simulation("accurate", precision, leaf_cap=leaf)
         ens.upload(bodies, offsets=offs)
         a = ens.accel()
