@@ -202,13 +202,63 @@ def run_reference_arm(args):
 
 
 CONFIGS = {
-    "c1": dict(name="plummer_16k", maker="plummer", n=16_384, seed=0, eps=0.01, theta=0.5, dt=1e-3),
+    "c1": dict(name="plummer_16k", maker="plummer", n=16_384, seed=0, eps=0.01, theta=0.5, dt=1e-3, steps=100),
     "c2": dict(name="cold_collapse_uniform_sphere", maker="uniform_sphere", n=1_048_576, seed=1, eps=0.005,
-               theta=0.5, dt=5e-4),
-    "c3": dict(name="two_galaxy_encounter", maker="two_galaxies", n=4_194_304, seed=2, eps=0.01, theta=0.6, dt=1e-3),
-    "c4": dict(name="batched_plummer_ensemble_256", maker="ensemble", n=None, seed=3, eps=0.01, theta=0.5, dt=1e-3),
-    "c5": dict(name="hernquist_halo_16M", maker="hernquist", n=16_777_216, seed=4, eps=0.002, theta=0.7, dt=2.5e-4),
+               theta=0.5, dt=5e-4, steps=200),
+    "c3": dict(name="two_galaxy_encounter", maker="two_galaxies", n=4_194_304, seed=2, eps=0.01, theta=0.6, dt=1e-3,
+               steps=100),
+    "c4": dict(name="batched_plummer_ensemble_256", maker="ensemble", n=None, seed=3, eps=0.01, theta=0.5, dt=1e-3,
+               steps=100),
+    "c5": dict(name="hernquist_halo_16M", maker="hernquist", n=16_777_216, seed=4, eps=0.002, theta=0.7, dt=2.5e-4,
+               steps=50),
 }
+
+
+def full_run(args):
+    """The workload's whole configured run (its step count and dt) from the
+    initial bodies through next_steps -- one graph replay per step, device
+    error word checked every 64 replays with overflow recovery -- reporting
+    completion, device time and the FP64 energy / momentum drift."""
+    from next_b200.native import Simulation
+    W = dict(CONFIGS[args.config])
+    bodies, offsets = make_bodies(W)
+    n = bodies["x"].shape[0]
+    precision = args.precision
+    sim = Simulation("accurate", precision, theta=W["theta"], eps=W["eps"])
+    sim.upload(bodies, offsets=offsets)
+    tune = sim.autotune()                        # positions unchanged
+    d0 = sim.diagnostics()
+    m = bodies["m"]
+    pscale = float(np.sum(m * np.sqrt(bodies["vx"] ** 2 + bodies["vy"] ** 2 + bodies["vz"] ** 2)))
+    sim.sync()
+    sim.reset_timers()
+    sim.set_timing(True)
+    t0 = time.perf_counter()
+    sim.steps(W["dt"], W["steps"])
+    sim.sync()
+    wall = time.perf_counter() - t0
+    sim.set_timing(False)
+    st = sim.stats()
+    d1 = sim.diagnostics()
+    e0, e1 = d0["kinetic"] + d0["potential"], d1["kinetic"] + d1["potential"]
+    final = {k: v for k, v in sim.download().items()}
+    vmag = np.sqrt(final["vx"] ** 2 + final["vy"] ** 2 + final["vz"] ** 2)
+    pscale = max(pscale, float(np.sum(m * vmag)))
+    err = None
+    if offsets is None:
+        idx = np.random.default_rng(12345).choice(n, min(4096, n), replace=False)
+        err = force_error(sim.accel(), sim.direct_accel(idx), idx)
+    sim.close()
+    line = {"full_run": W["name"], "precision": precision, "n_bodies": n, "steps": W["steps"], "dt": W["dt"],
+            "completed": st["steps"] == W["steps"] and st["device_error"] == 0,
+            "device_ms": st["ms_step"], "ms_per_step": st["ms_step"] / max(1, st["steps"]), "wall_s": wall,
+            "particle_steps_per_s": n * W["steps"] / (st["ms_step"] * 1e-3),
+            "energy": {"E0": e0, "E1": e1, "rel_drift": abs(e1 - e0) / abs(e0), "T1_over_W1": d1["kinetic"] / abs(d1["potential"])},
+            "momentum_drift": float(np.linalg.norm(d1["momentum"] - d0["momentum"])) / pscale,
+            "recoveries": st["recoveries"], "key_levels": st["key_levels"], "force_error_end": err,
+            "autotune": tune}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def make_bodies(cfg):
@@ -638,6 +688,9 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-large-sort", action="store_true")
+    ap.add_argument("--full-run", action="store_true",
+                    help="integrate the config's whole run (its step count) and report drift, not the bench line")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64group"], help="with --full-run")
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS), help="workload (default c2, the metric's)")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--n", type=int, default=None, help="override the body count of a single-system config")
@@ -650,6 +703,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.full_run:
+        return full_run(args)
     return run_ours(args)
 
 
