@@ -154,9 +154,17 @@ int next_steps(next_handle* h, double dt, int nsteps);
 /* The reference's Step(ParticleSystem&, dt) on host arrays (src/gravity/
  * step.h:25): upload x..vz, m and type (type may be NULL), one KDK step, and
  * the new positions and velocities written back into x..vz in place.  The
- * same as next_upload + next_step + next_download, but the positions are
- * copied back while the force phase runs.  Returns after every copy into
- * the caller's arrays has finished. */
+ * same as next_upload + next_step + next_download, but faster:
+ *  - the positions are copied back while the force phase runs;
+ *  - when the previous call on this handle was next_step_host with the same
+ *    n and nothing changed the held state since, the step starts on the held
+ *    state while the inputs upload, and the inputs are then compared bit for
+ *    bit with what that call returned (masses and types with what it was
+ *    given).  If they differ, the step is taken again from the inputs.
+ * Either way the result is the step of the inputs.  Returns after every copy
+ * into the caller's arrays has finished.  Inputs that are rejected
+ * (NEXT_ERR_INVALID_ARGUMENT: non-finite values, negative masses) leave
+ * x..vz as the caller passed them and the held state as it was. */
 int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, double* z,
                    double* vx, double* vy, double* vz, const double* m, const int* type);
 

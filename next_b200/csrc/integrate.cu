@@ -220,13 +220,38 @@ __global__ void load_all_kernel(const double* __restrict__ stage, const int* __r
     b.ax[i] = 0.0; b.ay[i] = 0.0; b.az[i] = 0.0;
 }
 
-// Download support: gather `count` FP64 lanes into caller order.
-__global__ void gather_out_kernel(const double* const* __restrict__ lanes, int count,
-                                  const uint32_t* __restrict__ inv, int64_t n, double* __restrict__ out) {
+// next_step_host's check that a call's inputs are the state the previous
+// call returned: positions and velocities against that call's export,
+// masses and types against its upload (all in caller order), bit for bit and
+// finite.  flags[0] = 1 on any difference.
+__global__ void same_as_last_kernel(const double* __restrict__ in, const int* __restrict__ type,
+                                    const double* __restrict__ prev_out, const double* __restrict__ prev_in,
+                                    const int* __restrict__ prev_type, int64_t n, int* flags) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool same = type[i] == prev_type[i];
+    for (int c = 0; c < 6; ++c) {
+        const double v = in[c * n + i];
+        same &= isfinite(v) && __double_as_longlong(v) == __double_as_longlong(prev_out[c * n + i]);
+    }
+    const double m = in[6 * n + i];
+    same &= isfinite(m) && __double_as_longlong(m) == __double_as_longlong(prev_in[6 * n + i]);
+    if (!same) flags[0] = 1;
+}
+
+// Download support: gather `count` FP64 lanes into caller order.  The lane
+// pointers travel by value in the launch, so no host-to-device copy of a
+// pointer table precedes the gather.
+struct LaneTable {
+    const double* p[kMaxGatherLanes];
+};
+
+__global__ void gather_out_kernel(LaneTable lanes, int count, const uint32_t* __restrict__ inv, int64_t n,
+                                  double* __restrict__ out) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t p = inv[i];
-    for (int c = 0; c < count; ++c) out[c * n + i] = lanes[c][p];
+    for (int c = 0; c < count; ++c) out[c * n + i] = lanes.p[c][p];
 }
 
 __global__ void ids_to_positions_kernel(const int64_t* __restrict__ ids, const uint32_t* __restrict__ inv, int64_t k,
@@ -337,10 +362,21 @@ cudaError_t launch_load_all(const double* stage, const int* stype, const Bodies&
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather_out(const double* const* lanes_dev, int count, const uint32_t* inv, int64_t n,
-                              double* out, cudaStream_t st) {
+cudaError_t launch_same_as_last(const double* in, const int* type, const double* prev_out, const double* prev_in,
+                                const int* prev_type, int64_t n, int* flags, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
-    gather_out_kernel<<<grid_for(n, 256), 256, 0, st>>>(lanes_dev, count, inv, n, out);
+    same_as_last_kernel<<<grid_for(n, 256), 256, 0, st>>>(in, type, prev_out, prev_in, prev_type, n, flags);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_out(const double* const* lanes, int count, const uint32_t* inv, int64_t n, double* out,
+                              cudaStream_t st) {
+    if (n <= 0 || count <= 0) return cudaSuccess;
+    if (count > kMaxGatherLanes) return cudaErrorInvalidValue;
+    LaneTable table{};
+    for (int c = 0; c < count; ++c) table.p[c] = lanes[c];
+    gather_out_kernel<<<grid_for(n, 256), 256, 0, st>>>(table, count, inv, n, out);
     count_launches(1);
     return cudaGetLastError();
 }

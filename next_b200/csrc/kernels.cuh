@@ -78,7 +78,13 @@ cudaError_t launch_load_velocities(const double* stage, const Bodies& b, const u
                                    cudaStream_t st);
 cudaError_t launch_load_all(const double* stage, const int* stype, const Bodies& b, uint32_t* inv, int64_t n,
                             cudaStream_t st);
-cudaError_t launch_gather_out(const double* const* lanes_dev, int count, const uint32_t* inv, int64_t n, double* out,
+// flags[0] = 1 unless in (7 lanes x n, caller order) and type equal prev_out's
+// 6 lanes, prev_in's mass lane and prev_type bit for bit (and are finite)
+cudaError_t launch_same_as_last(const double* in, const int* type, const double* prev_out, const double* prev_in,
+                                const int* prev_type, int64_t n, int* flags, cudaStream_t st);
+// gathers `count` (<= kMaxGatherLanes) lanes, given as host-side pointers to device arrays
+constexpr int kMaxGatherLanes = 8;
+cudaError_t launch_gather_out(const double* const* lanes, int count, const uint32_t* inv, int64_t n, double* out,
                               cudaStream_t st);
 cudaError_t launch_ids_to_positions(const int64_t* ids, const uint32_t* inv, int64_t k, int64_t* pos,
                                     cudaStream_t st);

@@ -58,9 +58,15 @@ namespace {
 
 constexpr int kWalkUnroll = NB_WALK_UNROLL;
 constexpr int kWalkGenericUnroll = NB_WALK_GENERIC_UNROLL;
-constexpr int kPcCap = 64;
+// Entries per evaluation batch (32 or 64): every lane stages kBatch / 32.
+#ifndef NB_WALK_BATCH
+#define NB_WALK_BATCH 64
+#endif
+constexpr int kBatch = NB_WALK_BATCH;
+static_assert(kBatch == 32 || kBatch == 64, "evaluation batches of 32 or 64 entries");
+constexpr int kPcCap = kBatch + 32;
 constexpr int kPpChunk = 16;
-constexpr int kPpCap = 32 + 32 * kPpChunk;
+constexpr int kPpCap = kBatch + 32 * kPpChunk;
 
 // Per-warp shared lists; STAGE_BYTES hold one staged evaluation batch.
 template <int STAGE_BYTES>
@@ -176,8 +182,8 @@ __device__ __forceinline__ void eval_batch(const float4* stage, int count, float
                                            int nslices, Target& T) {
     if (!active) return;
     float sx = 0.f, sy = 0.f, sz = 0.f, sp = 0.f;
-    if (NB_WALK_FIXED && count == 32 && nslices == 1) {
-        run_fixed<32, STRIDE, PC, F1, POT>(stage, 0, T, eps2, sx, sy, sz, sp);
+    if (NB_WALK_FIXED && count == kBatch && nslices == 1) {
+        run_fixed<kBatch, STRIDE, PC, F1, POT>(stage, 0, T, eps2, sx, sy, sz, sp);
     } else {
         const int chunk = (count + nslices - 1) / nslices;
         const int k0 = slice * chunk;
@@ -298,8 +304,8 @@ __device__ __forceinline__ void eval_batch_packed(const float4* stage, int count
     const f2 e2 = pk(eps2, eps2), neg25 = pk(-2.5f, -2.5f);
     PairAcc s{0ull, 0ull, 0ull};
     const int npairs = (count + 1) >> 1;
-    if (NB_WALK_FIXED && npairs == 16 && nslices == 1) {
-        run_pairs_fixed<16, STRIDE, PC, QUAD>(stage, 0, tx, ty, tz, e2, neg25, s);
+    if (NB_WALK_FIXED && npairs == kBatch / 2 && nslices == 1) {
+        run_pairs_fixed<kBatch / 2, STRIDE, PC, QUAD>(stage, 0, tx, ty, tz, e2, neg25, s);
     } else {
         const int chunk = (npairs + nslices - 1) / nslices;
         const int p0 = slice * chunk;
@@ -315,45 +321,51 @@ __device__ __forceinline__ void eval_batch_packed(const float4* stage, int count
     kahan_add(T.az, T.cz, sz.x + sz.y);
 }
 
-// Stage up to 32 cells of `list` (one per lane) as a packed batch: pairs of
-// entries interleaved field by field, 5 float4 per pair; lanes past `count`
-// stage zero-mass entries.  Positions are FP64 COM minus the FP64 group
-// centre, rounded to FP32.
+// Stage up to kBatch cells of `list` (entries lane, lane + 32, ...) as a
+// packed batch: pairs of entries interleaved field by field, 5 float4 per
+// pair; entries past `count` are zero-mass.  Positions are FP64 COM minus the
+// FP64 group centre, rounded to FP32.
 template <bool QUAD>
 __device__ __forceinline__ void stage_pc_packed(float4* stage, const int* list, int count, const Tree& t, double gcx,
                                                 double gcy, double gcz, float G, int lane) {
-    float* f = reinterpret_cast<float*>(stage + 5 * (lane >> 1)) + (lane & 1);
-    float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (lane < count) {
-        const int node = list[lane];
-        const double4 c = t.com[node];
-        v[0] = static_cast<float>(c.x - gcx);
-        v[1] = static_cast<float>(c.y - gcy);
-        v[2] = static_cast<float>(c.z - gcz);
-        v[3] = static_cast<float>(G * c.w);
-        if (QUAD) {
-            const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
-            v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
-        }
-    }
 #pragma unroll
-    for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+    for (int e = lane; e < kBatch; e += 32) {
+        float* f = reinterpret_cast<float*>(stage + 5 * (e >> 1)) + (e & 1);
+        float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        if (e < count) {
+            const int node = list[e];
+            const double4 c = t.com[node];
+            v[0] = static_cast<float>(c.x - gcx);
+            v[1] = static_cast<float>(c.y - gcy);
+            v[2] = static_cast<float>(c.z - gcz);
+            v[3] = static_cast<float>(G * c.w);
+            if (QUAD) {
+                const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
+                v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+    }
 }
 
-// Stage up to 32 bodies of `list` as a packed batch, 2 float4 per pair.
+// Stage up to kBatch bodies of `list` as a packed batch, 2 float4 per pair.
 __device__ __forceinline__ void stage_pp_packed(float4* stage, const int* list, int count, const Bodies& bd,
                                                 double gcx, double gcy, double gcz, float G, int lane) {
-    float* f = reinterpret_cast<float*>(stage + 2 * (lane >> 1)) + (lane & 1);
-    float v[4] = {0, 0, 0, 0};
-    if (lane < count) {
-        const int j = list[lane];
-        v[0] = static_cast<float>(bd.x[j] - gcx);
-        v[1] = static_cast<float>(bd.y[j] - gcy);
-        v[2] = static_cast<float>(bd.z[j] - gcz);
-        v[3] = static_cast<float>(G * bd.m[j]);
-    }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+    for (int e = lane; e < kBatch; e += 32) {
+        float* f = reinterpret_cast<float*>(stage + 2 * (e >> 1)) + (e & 1);
+        float v[4] = {0, 0, 0, 0};
+        if (e < count) {
+            const int j = list[e];
+            v[0] = static_cast<float>(bd.x[j] - gcx);
+            v[1] = static_cast<float>(bd.y[j] - gcy);
+            v[2] = static_cast<float>(bd.z[j] - gcz);
+            v[3] = static_cast<float>(G * bd.m[j]);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+    }
 }
 
 // Stage up to 32 cells (one per lane) and evaluate them.  PACK stages them in
@@ -367,21 +379,21 @@ __device__ __forceinline__ void eval_pc(float4* stage, const int* list, int coun
         __syncwarp();
         eval_batch_packed<5, true, QUAD>(stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
-        return;
-    }
-    if (lane < count) {
-        const int node = list[lane];
-        const double4 c = t.com[node];
-        stage[3 * lane + 0] = make_float4(static_cast<float>(c.x - gcx), static_cast<float>(c.y - gcy),
-                                          static_cast<float>(c.z - gcz), static_cast<float>(G * c.w));
-        if (QUAD) {
-            stage[3 * lane + 1] = t.quad32[2 * node];
-            stage[3 * lane + 2] = t.quad32[2 * node + 1];
+    } else {
+        for (int e = lane; e < count; e += 32) {
+            const int node = list[e];
+            const double4 c = t.com[node];
+            stage[3 * e + 0] = make_float4(static_cast<float>(c.x - gcx), static_cast<float>(c.y - gcy),
+                                           static_cast<float>(c.z - gcz), static_cast<float>(G * c.w));
+            if (QUAD) {
+                stage[3 * e + 1] = t.quad32[2 * node];
+                stage[3 * e + 2] = t.quad32[2 * node + 1];
+            }
         }
+        __syncwarp();
+        eval_batch<3, true, QUAD, POT>(stage, count, eps2, active, slice, nslices, T);
+        __syncwarp();
     }
-    __syncwarp();
-    eval_batch<3, true, QUAD, POT>(stage, count, eps2, active, slice, nslices, T);
-    __syncwarp();
 }
 
 // Stage up to 32 bodies (one per lane) and evaluate them.
@@ -394,16 +406,16 @@ __device__ __forceinline__ void eval_pp(float4* stage, const int* list, int coun
         __syncwarp();
         eval_batch_packed<2, false, false>(stage, count, eps2, active, slice, nslices, T);
         __syncwarp();
-        return;
+    } else {
+        for (int e = lane; e < count; e += 32) {
+            const int j = list[e];
+            stage[e] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
+                                   static_cast<float>(bd.z[j] - gcz), static_cast<float>(G * bd.m[j]));
+        }
+        __syncwarp();
+        eval_batch<1, false, SOFT, POT>(stage, count, eps2, active, slice, nslices, T);
+        __syncwarp();
     }
-    if (lane < count) {
-        const int j = list[lane];
-        stage[lane] = make_float4(static_cast<float>(bd.x[j] - gcx), static_cast<float>(bd.y[j] - gcy),
-                                  static_cast<float>(bd.z[j] - gcz), static_cast<float>(G * bd.m[j]));
-    }
-    __syncwarp();
-    eval_batch<1, false, SOFT, POT>(stage, count, eps2, active, slice, nslices, T);
-    __syncwarp();
 }
 
 // ---- the two arithmetics of the walk -----------------------------------------
@@ -415,7 +427,7 @@ struct MixedArith {
     using Scalar = float;
     // softened forces without the potential take the packed two-entry path
     static constexpr bool kPack = NB_WALK_PACKED && SOFT && !POT;
-    static constexpr int kStageBytes = 3 * 32 * sizeof(float4);
+    static constexpr int kStageBytes = 3 * kBatch * sizeof(float4);
     static constexpr int kMinBlocks = NB_WALK_MIN_BLOCKS;
     static constexpr bool kPot = POT;
     using Acc = Target;
@@ -449,7 +461,7 @@ struct MixedArith {
 template <bool QUAD, bool SOFT, bool POT>
 struct Fp64Arith {
     using Scalar = double;
-    static constexpr int kStageBytes = 32 * 10 * sizeof(double);
+    static constexpr int kStageBytes = kBatch * 10 * sizeof(double);
     static constexpr int kMinBlocks = NB_WALK64_MIN_BLOCKS;
     static constexpr bool kPot = POT;
     struct Acc {
@@ -515,15 +527,15 @@ struct Fp64Arith {
                               double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
                               int nslices, Acc& A, int lane) {
         double* st = reinterpret_cast<double*>(stage);
-        if (lane < count) {
-            const int node = list[lane];
+        for (int k = lane; k < count; k += 32) {
+            const int node = list[k];
             const double4 c = t.com[node];
-            double* e = st + 10 * lane;
+            double* e = st + 10 * k;
             e[0] = c.x - gcx; e[1] = c.y - gcy; e[2] = c.z - gcz; e[3] = G * c.w;
             if (QUAD) {
                 const double* q = t.quad64 + 8 * static_cast<int64_t>(node);
 #pragma unroll
-                for (int k = 0; k < 6; ++k) e[4 + k] = -G * q[k];
+                for (int f = 0; f < 6; ++f) e[4 + f] = -G * q[f];
             }
         }
         __syncwarp();
@@ -534,9 +546,9 @@ struct Fp64Arith {
                               double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
                               int nslices, Acc& A, int lane) {
         double* st = reinterpret_cast<double*>(stage);
-        if (lane < count) {
-            const int j = list[lane];
-            double* e = st + 4 * lane;
+        for (int k = lane; k < count; k += 32) {
+            const int j = list[k];
+            double* e = st + 4 * k;
             e[0] = bd.x[j] - gcx; e[1] = bd.y[j] - gcy; e[2] = bd.z[j] - gcz; e[3] = G * bd.m[j];
         }
         __syncwarp();
@@ -654,12 +666,12 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
             sp += total;
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
-            if (pc_n >= 32) {
-                A::pc(L.stage, L.pc, 32, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
+            if (pc_n >= kBatch) {
+                A::pc(L.stage, L.pc, kBatch, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
                       nslices, T, lane);
-                g_pc += 32;
-                pc_n -= 32;
-                const int v = lane < pc_n ? L.pc[32 + lane] : 0;
+                g_pc += kBatch;
+                pc_n -= kBatch;               // < 32 left over
+                const int v = lane < pc_n ? L.pc[kBatch + lane] : 0;
                 __syncwarp();
                 if (lane < pc_n) L.pc[lane] = v;
                 __syncwarp();
@@ -676,18 +688,21 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
                 remaining -= take;
                 __syncwarp();
                 int head = 0;
-                while (pp_n - head >= 32) {
-                    A::pp(L.stage, L.pp + head, 32, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active,
-                          slice, nslices, T, lane);
-                    g_pp += 32;
-                    head += 32;
+                while (pp_n - head >= kBatch) {
+                    A::pp(L.stage, L.pp + head, kBatch, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2,
+                          active, slice, nslices, T, lane);
+                    g_pp += kBatch;
+                    head += kBatch;
                 }
                 if (head > 0) {
-                    pp_n -= head;
-                    const int v = lane < pp_n ? L.pp[head + lane] : 0;
-                    __syncwarp();
-                    if (lane < pp_n) L.pp[lane] = v;
-                    __syncwarp();
+                    pp_n -= head;                 // < kBatch left over
+#pragma unroll
+                    for (int e0 = 0; e0 < kBatch; e0 += 32) {
+                        const int v = e0 + lane < pp_n ? L.pp[head + e0 + lane] : 0;
+                        __syncwarp();
+                        if (e0 + lane < pp_n) L.pp[e0 + lane] = v;
+                        __syncwarp();
+                    }
                 }
             }
         }

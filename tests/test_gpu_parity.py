@@ -542,6 +542,71 @@ def test_step_host_rejects_bad_input():
     h.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_step_host_with_changed_or_bad_inputs_between_calls(precision):
+    """next_step_host starts each step on the state it returned last time
+    while the new inputs upload, and keeps the result only if the inputs are
+    that state bit for bit.  Unchanged inputs give what upload + step +
+    download gives on a handle that holds the same state; inputs changed
+    between calls (one velocity, one mass, one position by an ulp, a zero's
+    sign) give the step of the changed state, equal to a new handle's upload +
+    step + download of it; a call with bad inputs fails, writes nothing back
+    and leaves the held state as the previous call returned it."""
+    b = ic.plummer(20_000, seed=14)
+    names = ("x", "y", "z", "vx", "vy", "vz", "m")
+    lanes = [np.ascontiguousarray(b[k], dtype=np.float64).copy() for k in names]
+    types = np.zeros(20_000, dtype=np.int32)
+    h = Simulation("accurate", precision)
+    ref = {}
+
+    def fresh():
+        # a new handle given the caller's current arrays
+        f = Simulation("accurate", precision)
+        for i, k in enumerate(names):
+            ref[k] = lanes[i].copy()
+        f.upload_arrays([ref[k] for k in names], types)
+        return f
+
+    def step_both(s):
+        s.upload_arrays([ref[k] for k in names], types)
+        s.step(1e-3)
+        s.download(ref)
+        h.step_host(lanes, 1e-3, types)
+        for i, k in enumerate(names[:6]):
+            np.testing.assert_array_equal(lanes[i], ref[k])
+
+    s = fresh()
+    step_both(s)
+    step_both(s)                          # unchanged inputs: the speculative step is kept
+    step_both(s)
+    edits = [lambda: lanes[3].__setitem__(17, lanes[3][17] + 1e-3),
+             lambda: lanes[6].__setitem__(400, lanes[6][400] * 1.5),
+             lambda: lanes[2].__setitem__(1, np.nextafter(lanes[2][1], 1.0)),
+             lambda: lanes[6].__setitem__(7, 0.0),
+             lambda: lanes[6].__setitem__(7, -0.0)]          # the sign of a zero mass alone
+    for edit in edits:
+        edit()
+        s.close()
+        s = fresh()                       # the changed state, from scratch
+        step_both(s)
+        step_both(s)                      # and unchanged again afterwards
+    # bad input on a speculative call: error, nothing written back
+    keep = [a.copy() for a in lanes]
+    lanes[6][3] = -1.0
+    with pytest.raises(NextError):
+        h.step_host(lanes, 1e-3, types)
+    for a, k in zip(lanes[:6], keep[:6]):
+        np.testing.assert_array_equal(a, k)
+    lanes[6][3] = keep[6][3]
+    s.close()
+    s = fresh()                           # carries on from the state before the bad call
+    step_both(s)
+    step_both(s)
+    assert s.stats()["device_error"] == 0 and h.stats()["device_error"] == 0
+    s.close()
+    h.close()
+
+
 def test_reuse_forces_matches_recompute():
     b = ic.plummer(20_000, seed=10)
     r = Simulation("accurate", "fp64", leaf_cap=4, reuse_forces=True)
