@@ -110,6 +110,25 @@ __device__ __forceinline__ uint32_t digit_peers(int dig) {
 #ifndef NB_SORT_MINB
 #define NB_SORT_MINB 3
 #endif
+// Tile loads into registers: item k of lane l of warp w is pair
+// tile_base + (w * kItems + k) * 32 + l; pairs past n are padding keys that
+// rank after every real key of the tile and are never written out.
+__device__ __forceinline__ void load_tile(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                                          int64_t n, int tile, int w, int lane, uint64_t (&key)[kItems],
+                                          uint32_t (&val)[kItems]) {
+    const int64_t warp_base = static_cast<int64_t>(tile) * kTile + static_cast<int64_t>(w) * kItems * 32;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+        const int64_t g = warp_base + k * 32 + lane;
+        if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; }
+        else { key[k] = ~0ull; val[k] = 0u; }
+    }
+}
+
+// Persistent: a block takes tiles by ticket until none is left.  Once a
+// tile's pairs sit ranked in shared memory, the block takes its next ticket
+// and loads that tile into the registers the ranking has freed, so the load
+// runs while this tile waits on its look-back and writes itself out.
 __global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
@@ -118,124 +137,131 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.warp_hist[0][0])[i] = 0;
+    const int ntiles = static_cast<int>((n + kTile - 1) / kTile);
     if (threadIdx.x == 0) S.tile = static_cast<int>(atomicAdd(tile_ticket, 1u));
     __syncthreads();
-    const int tile = S.tile;
-    const int64_t tile_base = static_cast<int64_t>(tile) * kTile;
-    const int64_t warp_base = tile_base + static_cast<int64_t>(w) * kItems * 32;
-
+    int tile = S.tile;
     // Digits are re-extracted from the keys where needed: holding them (or
     // anything derived from them) across the passes costs more registers.
     uint64_t key[kItems];
     uint32_t val[kItems];
+    if (tile < ntiles) load_tile(keys_in, vals_in, n, tile, w, lane, key, val);
+    while (tile < ntiles) {
+        const int64_t tile_base = static_cast<int64_t>(tile) * kTile;
+        for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.warp_hist[0][0])[i] = 0;
+        __syncthreads();
+        // Per-warp digit counts first (fire-and-forget shared adds by each digit's
+        // lowest lane), so the tile's counts are published before the ranking.
+        const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const int64_t g = warp_base + k * 32 + lane;
-        if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; }
-        else { key[k] = ~0ull; val[k] = 0u; }
-    }
-    // Per-warp digit counts first (fire-and-forget shared adds by each digit's
-    // lowest lane), so the tile's counts are published before the ranking.
-    const uint32_t lt = (1u << lane) - 1u;
+        for (int k = 0; k < kItems; ++k) {
+            const int dk = static_cast<int>((key[k] >> shift) & dmask);
+            const uint32_t peers = digit_peers(dk);
+            S.peers[k][threadIdx.x] = peers;
+            if ((peers & lt) == 0) atomicAdd(&S.warp_hist[w][dk], static_cast<uint32_t>(__popc(peers)));
+        }
+        __syncthreads();
+        // Per digit d: exclusive prefix over warps and the tile count, published
+        // at once; the first look-back window is read now and consumed after the
+        // local scan and the ranking, which do not need it.
+        const int d = threadIdx.x;
+        uint32_t count = 0;
+        for (int ww = 0; ww < kWarps; ++ww) {
+            const uint32_t c = S.warp_hist[ww][d];
+            S.warp_hist[ww][d] = count;
+            count += c;
+        }
+        volatile uint32_t* vstat = status;
+        if (tile == 0) vstat[d] = kFlagInc | count;
+        else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
+        uint32_t win[kLookWindow];
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const int dk = static_cast<int>((key[k] >> shift) & dmask);
-        const uint32_t peers = digit_peers(dk);
-        S.peers[k][threadIdx.x] = peers;
-        if ((peers & lt) == 0) atomicAdd(&S.warp_hist[w][dk], static_cast<uint32_t>(__popc(peers)));
-    }
-    __syncthreads();
-    // Per digit d: exclusive prefix over warps and the tile count, published
-    // at once; the first look-back window is read now and consumed after the
-    // local scan and the ranking, which do not need it.
-    const int d = threadIdx.x;
-    uint32_t count = 0;
-    for (int ww = 0; ww < kWarps; ++ww) {
-        const uint32_t c = S.warp_hist[ww][d];
-        S.warp_hist[ww][d] = count;
-        count += c;
-    }
-    volatile uint32_t* vstat = status;
-    if (tile == 0) vstat[d] = kFlagInc | count;
-    else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
-    uint32_t win[kLookWindow];
+        for (int j = 0; j < kLookWindow; ++j)
+            win[j] = tile - 1 - j >= 0 ? vstat[static_cast<int64_t>(tile - 1 - j) * kRadix + d]
+                                       : static_cast<uint32_t>(kFlagInc);
+        // Exclusive scan of the tile counts over digits: warp scans + warp totals.
+        uint32_t inc = count;
 #pragma unroll
-    for (int j = 0; j < kLookWindow; ++j)
-        win[j] = tile - 1 - j >= 0 ? vstat[static_cast<int64_t>(tile - 1 - j) * kRadix + d] : static_cast<uint32_t>(kFlagInc);
-    // Exclusive scan of the tile counts over digits: warp scans + warp totals.
-    uint32_t inc = count;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += u;
+        }
+        if (lane == 31) S.warp_total[w] = inc;
+        __syncthreads();
+        uint32_t tile_start = inc - count;
+        for (int ww = 0; ww < w; ++ww) tile_start += S.warp_total[ww];
+        // warp_hist[w][d] becomes the first local slot of warp w's digit-d keys
+        for (int ww = 0; ww < kWarps; ++ww) S.warp_hist[ww][d] += tile_start;
+        __syncthreads();
+        // Warp-level multisplit in item order (stable: item k of every lane
+        // precedes item k+1, lanes in order within an item), scattering each key
+        // to its local slot as it is ranked.
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t u = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += u;
-    }
-    if (lane == 31) S.warp_total[w] = inc;
-    __syncthreads();
-    uint32_t tile_start = inc - count;
-    for (int ww = 0; ww < w; ++ww) tile_start += S.warp_total[ww];
-    // warp_hist[w][d] becomes the first local slot of warp w's digit-d keys
-    for (int ww = 0; ww < kWarps; ++ww) S.warp_hist[ww][d] += tile_start;
-    __syncthreads();
-    // Warp-level multisplit in item order (stable: item k of every lane
-    // precedes item k+1, lanes in order within an item), scattering each key
-    // to its local slot as it is ranked.
+        for (int k = 0; k < kItems; ++k) {
+            const int dk = static_cast<int>((key[k] >> shift) & dmask);
+            const uint32_t peers = S.peers[k][threadIdx.x];
+            const uint32_t base = S.warp_hist[w][dk];
+            const uint32_t pos = base + __popc(peers & lt);
+            __syncwarp();
+            if ((peers & lt) == 0) S.warp_hist[w][dk] = base + __popc(peers);
+            S.keys[pos] = key[k];
+            S.vals[pos] = val[k];
+            __syncwarp();
+        }
+        // the tile is ranked in shared memory: take the next ticket and start
+        // loading that tile into the registers it has freed
+        if (threadIdx.x == 0) S.tile = static_cast<int>(atomicAdd(tile_ticket, 1u));
+        __syncthreads();
+        const int next = S.tile;
+        if (next < ntiles) load_tile(keys_in, vals_in, n, next, w, lane, key, val);
+        // Decoupled look-back for digit d over the earlier tiles, a window of
+        // statuses per step: entries are taken in order, an entry without a
+        // flag yet is re-read alone (bounded), the first inclusive one ends it.
+        uint32_t excl = 0;
+        if (tile > 0) {
+            int pred = tile - 1;
+            bool done = false, timed_out = false;
+            while (!done) {
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const int dk = static_cast<int>((key[k] >> shift) & dmask);
-        const uint32_t peers = S.peers[k][threadIdx.x];
-        const uint32_t base = S.warp_hist[w][dk];
-        const uint32_t pos = base + __popc(peers & lt);
-        __syncwarp();
-        if ((peers & lt) == 0) S.warp_hist[w][dk] = base + __popc(peers);
-        S.keys[pos] = key[k];
-        S.vals[pos] = val[k];
-        __syncwarp();
-    }
-    // Decoupled look-back for digit d over the earlier tiles, a window of
-    // statuses per step: entries are taken in order, an entry without a
-    // flag yet is re-read alone (bounded), the first inclusive one ends it.
-    uint32_t excl = 0;
-    if (tile > 0) {
-        int pred = tile - 1;
-        bool done = false, timed_out = false;
-        while (!done) {
-#pragma unroll
-            for (int j = 0; j < kLookWindow; ++j) {
-                if (done) break;
-                uint32_t v = win[j];
-                int spins = 0;
-                while ((v & (kFlagAgg | kFlagInc)) == 0) {
-                    if (++spins > kSpinLimit) { timed_out = true; break; }
-                    v = vstat[static_cast<int64_t>(pred - j) * kRadix + d];
+                for (int j = 0; j < kLookWindow; ++j) {
+                    if (done) break;
+                    uint32_t v = win[j];
+                    int spins = 0;
+                    while ((v & (kFlagAgg | kFlagInc)) == 0) {
+                        if (++spins > kSpinLimit) { timed_out = true; break; }
+                        v = vstat[static_cast<int64_t>(pred - j) * kRadix + d];
+                    }
+                    excl += v & kCountMask;
+                    done = (v & kFlagInc) || timed_out || pred - j == 0;
                 }
-                excl += v & kCountMask;
-                done = (v & kFlagInc) || timed_out || pred - j == 0;
+                if (done) break;
+                pred -= kLookWindow;
+#pragma unroll
+                for (int j = 0; j < kLookWindow; ++j)
+                    win[j] = pred - j >= 0 ? vstat[static_cast<int64_t>(pred - j) * kRadix + d]
+                                           : static_cast<uint32_t>(kFlagInc);
             }
-            if (done) break;
-            pred -= kLookWindow;
-#pragma unroll
-            for (int j = 0; j < kLookWindow; ++j)
-                win[j] = pred - j >= 0 ? vstat[static_cast<int64_t>(pred - j) * kRadix + d] : static_cast<uint32_t>(kFlagInc);
+            if (timed_out) raise_error(err, kErrSort);
+            vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
         }
-        if (timed_out) raise_error(err, kErrSort);
-        vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagInc | ((excl + count) & kCountMask);
-    }
-    // global position of local slot i with digit d: global_delta[d] + i
-    S.global_delta[d] = digit_offsets[d] + excl - tile_start;
-    __syncthreads();
-    const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
+        // global position of local slot i with digit d: global_delta[d] + i
+        S.global_delta[d] = digit_offsets[d] + excl - tile_start;
+        __syncthreads();
+        const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-        const int i = k * kThreads + threadIdx.x;
-        if (i < valid) {
-            const uint64_t kk = S.keys[i];
-            const int dd = static_cast<int>((kk >> shift) & dmask);
-            const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
-            if (gpos >= n) { raise_error(err, kErrIndex); continue; }
-            keys_out[gpos] = kk;
-            vals_out[gpos] = S.vals[i];
+        for (int k = 0; k < kItems; ++k) {
+            const int i = k * kThreads + threadIdx.x;
+            if (i < valid) {
+                const uint64_t kk = S.keys[i];
+                const int dd = static_cast<int>((kk >> shift) & dmask);
+                const uint32_t gpos = S.global_delta[dd] + static_cast<uint32_t>(i);
+                if (gpos >= n) { raise_error(err, kErrIndex); continue; }
+                keys_out[gpos] = kk;
+                vals_out[gpos] = S.vals[i];
+            }
         }
+        __syncthreads();          // shared memory is reused by the next tile
+        tile = next;
     }
 }
 
@@ -248,6 +274,25 @@ size_t sort_scratch_words(int64_t n) {
 }
 
 size_t sort_smem_bytes() { return sizeof(SortSmem); }
+
+#ifndef NB_SORT_PERSISTENT
+#define NB_SORT_PERSISTENT 1
+#endif
+
+// Blocks of one onesweep pass: every tile's own block, or (persistent) no
+// more than fit on the device at once, each taking tiles until none is left.
+static unsigned onesweep_grid(int64_t tiles) {
+    if (!NB_SORT_PERSISTENT) return static_cast<unsigned>(tiles);
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kThreads, sizeof(SortSmem)) !=
+            cudaSuccess ||
+        per_sm < 1 || sms < 1)
+        return static_cast<unsigned>(tiles);
+    const int64_t resident = static_cast<int64_t>(per_sm) * sms;
+    return static_cast<unsigned>(tiles < resident ? tiles : resident);
+}
 
 cudaError_t sort_prepare() {
     return cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -278,7 +323,7 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
     uint64_t* src_k = keys; uint32_t* src_v = vals;
     uint64_t* dst_k = alt_keys; uint32_t* dst_v = alt_vals;
     for (int p = 0; p < passes; ++p) {
-        onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
+        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
             status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         uint64_t* tk = src_k; src_k = dst_k; dst_k = tk;
@@ -326,7 +371,7 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
         const bool to_out = ((passes - 1 - p) & 1) == 0;
         uint64_t* dst_k = to_out ? keys_out : alt_keys;
         uint32_t* dst_v = to_out ? vals_out : alt_vals;
-        onesweep_kernel<<<static_cast<unsigned>(tiles), kThreads, sizeof(SortSmem), st>>>(
+        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
             src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
             status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         src_k = dst_k;

@@ -18,7 +18,9 @@
 // Child bounds: one thread per internal cell runs the eight lower-bound
 // searches for the cell's end and child starts together.
 //
-// Upward pass: one thread per leaf computes the leaf's moments, then climbs;
+// Upward pass: one thread per leaf computes the leaf's moments (accurate
+// physics: in one pass over its bodies, moments about the first body shifted
+// to the centre of mass; reference physics: the reference's two passes), then climbs;
 // at each parent an atomic arrival counter elects the last child's thread to
 // combine all children in octant order (deterministic), and that thread
 // climbs on.  One launch, no per-level loop.
@@ -352,6 +354,9 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
 #ifndef NB_UP_MINB
 #define NB_UP_MINB 4
 #endif
+#ifndef NB_UP_ONEPASS
+#define NB_UP_ONEPASS 1
+#endif
 #if NB_UP_MINB > 0
 __global__ void __launch_bounds__(256, NB_UP_MINB)
 #else
@@ -385,6 +390,37 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                     return make_double4(bd.x[first + k], bd.y[first + k], bd.z[first + k], bd.m[first + k]);
                 });
             }
+        } else if (NB_UP_ONEPASS) {
+            // one pass over the leaf's bodies: mass, first and second moments
+            // about its first body (all of cell size, so no cancellation),
+            // then shifted to the centre of mass
+            const uint64_t key = cnt > 0 ? keys[first] : 0ull;
+            const double x0 = cnt > 0 ? bd.x[first] : 0.0, y0 = cnt > 0 ? bd.y[first] : 0.0,
+                         z0 = cnt > 0 ? bd.z[first] : 0.0;
+            double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+            for (int j = first; j < first + cnt; ++j) {
+                const double mj = bd.m[j];
+                const double dx = bd.x[j] - x0, dy = bd.y[j] - y0, dz = bd.z[j] - z0;
+                const double mx = mj * dx, my = mj * dy, mz = mj * dz;
+                m += mj; sx += mx; sy += my; sz += mz;
+                sxx += mx * dx; syy += my * dy; szz += mz * dz;
+                sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+            }
+            double cx, cy, cz;
+            if (m > 0) {
+                const double ox = sx / m, oy = sy / m, oz = sz / m;
+                cx = x0 + ox; cy = y0 + oy; cz = z0 + oz;
+                // second moments about the centre of mass
+                const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
+                const double tr = qxx + qyy + qzz;
+                a.q[0] = 3.0 * qxx - tr; a.q[1] = 3.0 * qyy - tr; a.q[2] = 3.0 * qzz - tr;
+                a.q[3] = 3.0 * (sxy - sx * oy); a.q[4] = 3.0 * (sxz - sx * oz); a.q[5] = 3.0 * (syz - sy * oz);
+            } else {
+                const double3 g = cell_centre(key, lvl, cube, base);
+                cx = g.x; cy = g.y; cz = g.z;
+            }
+            a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
+            rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
         } else {
             double m = 0, cx = 0, cy = 0, cz = 0;
             for (int j = first; j < first + cnt; ++j) {
