@@ -37,7 +37,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
 # capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
-WALK_DRAM_BYTES = 56.88e6
+WALK_DRAM_BYTES = 56.77e6
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -664,7 +664,8 @@ def run_ours(args):
         "roofline": {"bound": "fp32", "kernel": "walk_group_kernel<MixedArith<1,1,0>>", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      "traffic": WALK_DRAM_BYTES if args.config == "c2" else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this workload",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch of this workload "
+                                       "(profiles/walk_group_mixed_cold_collapse_1M.md)",
                      "peak_source": "measured live by next_fp32_peak (FFMA chains); MEASURED_PEAKS.json has no FP32 entry",
                      "flops_per_launch": flops_walk, "ms_per_launch": walk_ms,
                      "flops_rule": "20 per body-body + 56 per body-cell interaction"},
