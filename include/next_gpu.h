@@ -285,7 +285,9 @@ int next_get_params(const next_handle* h, next_params* p);
  *     it to the other ranks (e.g. over its own process group).
  *   next_dist_attach: joins the communicator (blocks until all ranks join).
  *     With id128 == NULL no communicator is made and the handle computes only
- *     its own share (one-device emulation of a rank, for tests).
+ *     its own share (one-device emulation of a rank, for tests).  world = 1
+ *     with an id makes a one-rank communicator: every force phase still runs
+ *     its all-gathers (trivially), which exercises the NCCL path on one GPU.
  * NCCL is loaded at run time (libnccl.so.2). */
 int next_dist_unique_id(unsigned char* id128);
 int next_dist_attach(next_handle* h, int rank, int world, const unsigned char* id128);

@@ -382,7 +382,7 @@ int walk(next_handle* h, bool potential) {
 }
 
 int exchange_forces(next_handle* h, bool potential) {
-    if (h->world <= 1 || !h->comm) return NEXT_OK;
+    if (!h->comm) return NEXT_OK;   // one rank with a communicator still runs the (trivial) all-gather
     const size_t chunk = static_cast<size_t>((h->n + h->world - 1) / h->world);
     double* lanes[4] = {h->ax, h->ay, h->az, h->pot};
     std::string why;
@@ -1690,7 +1690,7 @@ int next_dist_attach(next_handle* h, int rank, int world, const unsigned char* i
     drop_graphs(h);
     nccl_comm_destroy(h->comm);
     h->comm = nullptr;
-    if (world > 1 && id128) {
+    if (id128) {
         std::string why;
         if (!nccl_comm_init(&h->comm, rank, world, id128, &why)) return fail(h, NEXT_ERR_CUDA, why);
     }

@@ -18,12 +18,13 @@
 // Child bounds: one thread per internal cell runs the eight lower-bound
 // searches for the cell's end and child starts together.
 //
-// Upward pass: one thread per leaf computes the leaf's moments (accurate
-// physics: in one pass over its bodies, moments about the first body shifted
-// to the centre of mass; reference physics: the reference's two passes), then climbs;
+// Upward pass: one thread per leaf computes the leaf's moments, then climbs;
 // at each parent an atomic arrival counter elects the last child's thread to
 // combine all children in octant order (deterministic), and that thread
-// climbs on.  One launch, no per-level loop.
+// climbs on.  One launch, no per-level loop.  With accurate physics a leaf's
+// bodies and a cell's children are each read in one pass (moments about the
+// first one, shifted to the centre of mass by the parallel-axis rule); the
+// reference's physics keeps its own two-pass order for bit-exact moments.
 //
 // Built with -fmad=false: every FP64 + and * rounds separately, so the
 // reference-mode moments repeat src/gravity/octree.h:92-127 bit for bit.
@@ -357,6 +358,9 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
 #ifndef NB_UP_ONEPASS
 #define NB_UP_ONEPASS 1
 #endif
+#ifndef NB_UP_ONEPASS_CLIMB
+#define NB_UP_ONEPASS_CLIMB 1
+#endif
 #if NB_UP_MINB > 0
 __global__ void __launch_bounds__(256, NB_UP_MINB)
 #else
@@ -460,6 +464,7 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
             }
             if (old != plk.y - 1) break;
             t.counter[q] = 0;                      // re-armed for the next build
+            const int next_q = t.parent[nid];     // in flight beside the children's loads
             const int pl = rec.z >> 8;
             const int ps = rec.w;
             const double4 pcube = cubes[sysid ? sysid[ps] : 0];
@@ -468,6 +473,42 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
             double prc = 0.0;
             if (!accurate) {
                 p = combine_ref(plk.y, phalf, [&](int k) { return ldcg4(t.com + plk.x + k); });
+            } else if (NB_UP_ONEPASS_CLIMB) {
+                // one pass over the children: mass, first and second moments of
+                // their centres of mass about the first child's, their own
+                // quadrupoles; then shifted to the parent's centre of mass
+                // (parallel axes)
+                const double4 c0 = ldcg4(t.com + plk.x);
+                double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+                double qs[6] = {0, 0, 0, 0, 0, 0};
+                for (int k = 0; k < plk.y; ++k) {
+                    const double4 c = ldcg4(t.com + plk.x + k);
+                    const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
+                    const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
+                    const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
+                    m += c.w; sx += mx; sy += my; sz += mz;
+                    sxx += mx * dx; syy += my * dy; szz += mz * dz;
+                    sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+#pragma unroll
+                    for (int f = 0; f < 6; ++f) qs[f] += __ldcg(cq + f);
+                }
+                const uint64_t key = keys[ps];
+                double cx, cy, cz;
+                if (m > 0) {
+                    const double ox = sx / m, oy = sy / m, oz = sz / m;
+                    cx = c0.x + ox; cy = c0.y + oy; cz = c0.z + oz;
+                    const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
+                    const double tr = qxx + qyy + qzz;
+                    p.q[0] = qs[0] + (3.0 * qxx - tr); p.q[1] = qs[1] + (3.0 * qyy - tr);
+                    p.q[2] = qs[2] + (3.0 * qzz - tr); p.q[3] = qs[3] + 3.0 * (sxy - sx * oy);
+                    p.q[4] = qs[4] + 3.0 * (sxz - sx * oz); p.q[5] = qs[5] + 3.0 * (syz - sy * oz);
+                } else {
+                    const double3 g = cell_centre(key, pl, pcube, base);
+                    cx = g.x; cy = g.y; cz = g.z;
+                    for (int f = 0; f < 6; ++f) p.q[f] = qs[f];
+                }
+                p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
+                prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
             } else {
                 double m = 0, cx = 0, cy = 0, cz = 0;
                 for (int k = 0; k < plk.y; ++k) {
@@ -494,7 +535,7 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                 prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
             }
             store_moments(t, nid, p, phalf, prc, P.G, accurate);
-            q = t.parent[nid];
+            q = next_q;
         }
     }
 }

@@ -607,6 +607,34 @@ def test_step_host_with_changed_or_bad_inputs_between_calls(precision):
     h.close()
 
 
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_one_rank_nccl_exchange_is_bit_identical(precision):
+    """The sharded step's NCCL path on the one GPU a test gets: a one-rank
+    communicator (ncclCommInitRank through the run-time loaded libnccl), the
+    in-place all-gathers of every force phase -- eager and captured in the
+    step graphs -- and the padded force lanes.  The state equals an
+    unsharded handle's bit for bit."""
+    from next_b200.native import dist_unique_id
+    b = ic.plummer(20_000, seed=23)
+    ref = Simulation("accurate", precision)
+    one = Simulation("accurate", precision)
+    ref.upload(b)
+    one.upload(b)
+    one.dist_attach(0, 1, dist_unique_id())
+    for s_ in (ref, one):
+        s_.step(1e-3)
+        s_.steps(1e-3, 4)
+    a, c = ref.accel(), one.accel()
+    for k in ("ax", "ay", "az"):
+        np.testing.assert_array_equal(a[k], c[k])
+    sr, so = ref.download(), one.download()
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(sr[k], so[k])
+    assert one.stats()["device_error"] == 0
+    ref.close()
+    one.close()
+
+
 def test_reuse_forces_matches_recompute():
     b = ic.plummer(20_000, seed=10)
     r = Simulation("accurate", "fp64", leaf_cap=4, reuse_forces=True)
