@@ -1058,6 +1058,23 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
         h->io_ready = true;
         return NEXT_OK;
     }
+    // The step on the held state goes on st first: it runs while the host
+    // queues the upload, which for pageable caller arrays blocks the host
+    // until they are staged.  Its results go into the caller's arrays as soon
+    // as they are final and those arrays have been uploaded (positions beside
+    // the force phase, velocities after the closing kick), before the check
+    // has its verdict: the check's kernel may have to wait for the walk's
+    // resident blocks to finish.  If the verdict is "changed", the step is
+    // taken again from the upload and its results overwrite these; if the
+    // upload is invalid, the caller's arrays get the upload back.
+    rc = set_dt(h, dt);
+    if (rc) return rc;
+    bool pending = false;
+    rc = step_and_export(h, x, y, z, vx, vy, vz, out, false, &pending);
+    if (rc) {
+        NB_TRY(cudaStreamSynchronize(h->st), "sync");
+        return rc;
+    }
     // the upload and its check, on st_in
     const int p = h->io_cur;
     double* in = h->io_in[k];
@@ -1076,25 +1093,12 @@ int next_step_host(next_handle* h, double dt, int64_t n, double* x, double* y, d
     NB_TRY(launch_same_as_last(in, h->io_type[k], h->io_out[p], h->io_in[p], h->io_type[p], n, h->io_flag, h->st_in),
            "upload check");
     NB_TRY(cudaMemcpyAsync(h->h_flags + 3, h->io_flag, sizeof(int), cudaMemcpyDeviceToHost, h->st_in), "io flag");
-    // The step on the held state, on st.  Its results go into the caller's
-    // arrays as soon as they are final and those arrays have been uploaded
-    // (positions beside the force phase, velocities after the closing kick),
-    // before the check has its verdict: the check's kernel may have to wait
-    // for the walk's resident blocks to finish.  If the verdict is "changed",
-    // the step is taken again from the upload and its results overwrite
-    // these; if the upload is invalid, the caller's arrays get the upload back.
-    rc = set_dt(h, dt);
-    if (rc) return rc;
-    bool pending = false;
-    rc = step_and_export(h, x, y, z, vx, vy, vz, out, false, &pending);
-    if (rc == NEXT_OK) {
-        NB_TRY(cudaStreamWaitEvent(h->st_out, h->ev_out, 0), "export wait");
-        NB_TRY(cudaStreamWaitEvent(h->st_out, h->ev_in_pos, 0), "upload wait");
-        for (int c = 0; c < 3; ++c)
-            NB_TRY(cudaMemcpyAsync(xs[c], out + static_cast<int64_t>(c) * n, sizeof(double) * n,
-                                   cudaMemcpyDeviceToHost, h->st_out), "download");
-        rc = finish_and_export_velocities(h, vx, vy, vz, out, h->ev_in_vel);
-    }
+    NB_TRY(cudaStreamWaitEvent(h->st_out, h->ev_out, 0), "export wait");
+    NB_TRY(cudaStreamWaitEvent(h->st_out, h->ev_in_pos, 0), "upload wait");
+    for (int c = 0; c < 3; ++c)
+        NB_TRY(cudaMemcpyAsync(xs[c], out + static_cast<int64_t>(c) * n, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                               h->st_out), "download");
+    rc = finish_and_export_velocities(h, vx, vy, vz, out, h->ev_in_vel);
     const cudaError_t ei = cudaStreamSynchronize(h->st_in);
     const cudaError_t eo = cudaStreamSynchronize(h->st_out);
     const cudaError_t es = cudaStreamSynchronize(h->st);
@@ -1559,7 +1563,7 @@ int next_autotune(next_handle* h, next_tune_result* out) {
     struct Cand { int leaf, group, warps; };
     std::vector<Cand> cands;
     for (int g : {16, 24, 32})
-        for (int l : {8, 12, 16, 24})
+        for (int l : {8, 12, 16, 24, 32})
             for (int w : {2, 4})
                 if (l <= g) cands.push_back({l, g, w});
     // Small systems have fewer groups than the GPU has resident warps, and a
