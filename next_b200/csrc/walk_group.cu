@@ -50,7 +50,7 @@ namespace {
 #define NB_WALK_PACKED 1
 #endif
 #ifndef NB_WALK_MIN_BLOCKS
-#define NB_WALK_MIN_BLOCKS 6
+#define NB_WALK_MIN_BLOCKS 5
 #endif
 #ifndef NB_WALK64_MIN_BLOCKS
 #define NB_WALK64_MIN_BLOCKS 4
@@ -87,10 +87,11 @@ __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
     return inc - v;
 }
 
-// The walk runs at its register cap (6 blocks of 4 warps per SM): the FP64
-// group centre is read back from shared memory at each staging rather than
-// held in six registers across the evaluation loops (fewer spills, ~1 %).
-// The volatile read keeps the compiler from hoisting it back into registers.
+// The walk runs at its register cap (96 per thread: 5 blocks of 4 warps per
+// SM; with batches of 64 entries the extra registers of 5 blocks beat the
+// extra warps of 6).  The FP64 group centre is read back from shared memory
+// at each staging rather than held in six registers across the evaluation
+// loops; the volatile read keeps the compiler from hoisting it back.
 __device__ __forceinline__ double vld(const double& v) { return *reinterpret_cast<const volatile double*>(&v); }
 
 struct Target {
