@@ -49,6 +49,9 @@ namespace {
 #ifndef NB_WALK_PACKED
 #define NB_WALK_PACKED 1
 #endif
+#ifndef NB_WALK_PARTIAL_FIXED
+#define NB_WALK_PARTIAL_FIXED 1
+#endif
 #ifndef NB_WALK_MIN_BLOCKS
 #define NB_WALK_MIN_BLOCKS 5
 #endif
@@ -311,7 +314,12 @@ __device__ __forceinline__ void eval_batch_packed(const float4* stage, int count
         const int chunk = (npairs + nslices - 1) / nslices;
         const int p0 = slice * chunk;
         const int p1 = min(npairs, p0 + chunk);
-        for (int p = p0; p < p1; ++p) {
+        int p = p0;
+        // partial batches and slices: runs of 8 pairs with a compile-time
+        // trip count, then the rest one pair at a time
+        if (NB_WALK_PARTIAL_FIXED)
+            for (; p + 8 <= p1; p += 8) run_pairs_fixed<8, STRIDE, PC, QUAD>(stage, p, tx, ty, tz, e2, neg25, s);
+        for (; p < p1; ++p) {
             if (PC) pc_pair<QUAD>(stage + STRIDE * p, tx, ty, tz, e2, neg25, s);
             else pp_pair(stage + STRIDE * p, tx, ty, tz, e2, s);
         }
