@@ -217,7 +217,7 @@ int cuda_fail(next_handle* h, cudaError_t e, const char* where) {
 void free_tree(next_handle* h) {
     Tree& t = h->t;
     dfree(t.dlev); dfree(t.nint); dfree(t.int_start); dfree(t.int_level); dfree(t.int_bounds);
-    dfree(t.int_packed); dfree(t.int_node); dfree(t.counter); dfree(t.climb); dfree(t.link); dfree(t.parent); dfree(t.level);
+    dfree(t.int_packed); dfree(t.int_node); dfree(t.counter); dfree(t.climb); dfree(t.ready); dfree(t.link); dfree(t.parent); dfree(t.level);
     dfree(t.com); dfree(t.quad64); dfree(t.box); dfree(t.quad32); dfree(t.groups);
     dfree(h->scan_tmp);
     t.cap_int = t.cap_node = t.cap_group = 0;
@@ -245,6 +245,7 @@ int alloc_tree(next_handle* h, int64_t cap_int) {
     A(&t.dlev, n + 1); A(&t.nint, n + 1);
     A(&t.int_start, cap_int); A(&t.int_level, cap_int); A(&t.int_bounds, 9 * cap_int);
     A(&t.int_packed, cap_int + 1); A(&t.int_node, cap_int); A(&t.counter, cap_int); A(&t.climb, cap_int);
+    A(&t.ready, cap_int);
     A(&t.link, t.cap_node); A(&t.parent, t.cap_node); A(&t.level, t.cap_node);
     A(&t.com, t.cap_node); A(&t.quad64, 8 * t.cap_node);
     if (h->P.physics == NEXT_PHYSICS_ACCURATE) { A(&t.box, t.cap_node); A(&t.quad32, 2 * t.cap_node); }
@@ -731,12 +732,12 @@ int next_create(const next_params* p, next_handle** out) {
     auto A = [&](auto** q, size_t c) { if (e == cudaSuccess) e = dalloc(q, c); };
     A(&h->err, 1); A(&h->stats, 4); A(&h->queue, 1); A(&h->tickets, 4); A(&h->partial, kReduceMax * 8);
     A(&h->dts, 2); A(&h->dt_out, 2); A(&h->diag, 8); A(&h->changed, 4); A(&h->fma_out, 1);
-    A(&h->t.counts, 4); A(&h->done, 1);
+    A(&h->t.counts, 6); A(&h->done, 1);
     if (e != cudaSuccess) return bail(e, "scalars");
     e = cudaMemset(h->err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->tickets, 0, sizeof(unsigned int) * 4);
     if (e == cudaSuccess) e = cudaMemset(h->stats, 0, sizeof(unsigned long long) * 4);
-    if (e == cudaSuccess) e = cudaMemset(h->t.counts, 0, sizeof(int64_t) * 4);
+    if (e == cudaSuccess) e = cudaMemset(h->t.counts, 0, sizeof(int64_t) * 6);
     if (e == cudaSuccess) e = cudaMemset(h->done, 0, sizeof(unsigned int));
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_dts), sizeof(double) * 2, cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&h->h_err), sizeof(int) * 2, cudaHostAllocDefault);

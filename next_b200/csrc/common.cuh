@@ -68,7 +68,9 @@ struct Tree {
     float4* quad32;        // 2 per node: -G (Qxx Qyy Qzz Qxy) (Qxz Qyz 0 0)
     // walk groups
     int4* groups;          // (first body, count, root node, 0)
-    // device scalars: [0] internal count, [1] node count, [2] group count
+    int32_t* ready;        // upward pass: internal ids whose children are all leaves
+    // device scalars: [0] internal count, [1] node count, [2] group count,
+    // [3] deepest leaf level, [4] ready-list length
     int64_t* counts;
 };
 

@@ -41,21 +41,57 @@ __global__ void kick_drift_kernel(Bodies b, int64_t n, const double* __restrict_
 // The same kick-drift over a grid-stride loop that also boxes the drifted
 // positions: the last block to finish folds the block boxes into the root
 // cube the next build needs (one system), saving the build a pass over x, y, z.
+#ifndef NB_KDB_BATCH
+#define NB_KDB_BATCH 2
+#endif
 __global__ void __launch_bounds__(kBoxThreads)
 kick_drift_box_kernel(Bodies b, int64_t n, const double* __restrict__ dts, const int* err, double* __restrict__ partial,
                       unsigned int* ticket, double4* cube) {
     if (*err & kErrAbort) return;
     const double dt = dts[0], half = dts[1];
     double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
-        vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
-        b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
-        const double px = b.x[i] + vx * dt, py = b.y[i] + vy * dt, pz = b.z[i] + vz * dt;
-        b.x[i] = px; b.y[i] = py; b.z[i] = pz;
-        lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
-        lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
-        lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    if (NB_KDB_BATCH > 1) {
+        // NB_KDB_BATCH bodies per thread and round, all their loads issued
+        // before any store (the lanes' pointers may alias, so the compiler
+        // would not hoist a later body's loads above an earlier one's stores)
+        for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i0 < n; i0 += stride * NB_KDB_BATCH) {
+            double vx[NB_KDB_BATCH], vy[NB_KDB_BATCH], vz[NB_KDB_BATCH], ax[NB_KDB_BATCH], ay[NB_KDB_BATCH],
+                az[NB_KDB_BATCH], x[NB_KDB_BATCH], y[NB_KDB_BATCH], z[NB_KDB_BATCH];
+#pragma unroll
+            for (int u = 0; u < NB_KDB_BATCH; ++u) {
+                const int64_t i = i0 + u * stride;
+                if (i < n) {
+                    vx[u] = b.vx[i]; vy[u] = b.vy[i]; vz[u] = b.vz[i];
+                    ax[u] = b.ax[i]; ay[u] = b.ay[i]; az[u] = b.az[i];
+                    x[u] = b.x[i]; y[u] = b.y[i]; z[u] = b.z[i];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < NB_KDB_BATCH; ++u) {
+                const int64_t i = i0 + u * stride;
+                if (i < n) {
+                    const double wx = vx[u] + ax[u] * half, wy = vy[u] + ay[u] * half, wz = vz[u] + az[u] * half;
+                    b.vx[i] = wx; b.vy[i] = wy; b.vz[i] = wz;
+                    const double px = x[u] + wx * dt, py = y[u] + wy * dt, pz = z[u] + wz * dt;
+                    b.x[i] = px; b.y[i] = py; b.z[i] = pz;
+                    lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
+                    lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
+                    lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
+                }
+            }
+        }
+    } else {
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+            double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+            vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
+            b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
+            const double px = b.x[i] + vx * dt, py = b.y[i] + vy * dt, pz = b.z[i] + vz * dt;
+            b.x[i] = px; b.y[i] = py; b.z[i] = pz;
+            lo[0] = fmin(lo[0], px); hi[0] = fmax(hi[0], px);
+            lo[1] = fmin(lo[1], py); hi[1] = fmax(hi[1], py);
+            lo[2] = fmin(lo[2], pz); hi[2] = fmax(hi[2], pz);
+        }
     }
     block_minmax3(lo, hi);
     __shared__ bool last;

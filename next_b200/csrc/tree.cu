@@ -136,6 +136,9 @@ __global__ void cell_starts_kernel(const int8_t* __restrict__ dlev, const int32_
 // run together with one shared step sequence (the range halves every step
 // whatever the comparisons give), so a thread has eight independent loads in
 // flight per step and no divergence.
+#ifndef NB_INT_SCAN
+#define NB_INT_SCAN 128
+#endif
 __global__ void __launch_bounds__(256)
 internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int32_t* __restrict__ sysid,
                 const int64_t* __restrict__ offsets, int base, int levels, int leaf_cap, int group_cap, Tree t,
@@ -156,10 +159,27 @@ internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int32_t* __r
         v[0] = (prefix | low) + 1ull;                      // end of the cell
 #pragma unroll
         for (int c = 1; c < 8; ++c) v[c] = prefix | (static_cast<uint64_t>(c) << csh);
+        // A small cell's end is the first p > s whose key shares fewer than l
+        // digits with its predecessor (dlev[p] < l): found by reading dlev
+        // forward, 16 positions per round trip, for up to NB_INT_SCAN
+        // positions; the children's searches then run over the cell only.
+        int64_t e = -1;
+        if (NB_INT_SCAN > 0) {
+            const int64_t lim = hi < static_cast<int64_t>(s) + 1 + NB_INT_SCAN ? hi : static_cast<int64_t>(s) + 1 + NB_INT_SCAN;
+            for (int64_t p0 = static_cast<int64_t>(s) + 1; p0 < lim && e < 0; p0 += 16) {
+                int dv[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) dv[j] = p0 + j < lim ? t.dlev[p0 + j] : 127;
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    if (e < 0 && dv[j] < l) e = p0 + j;
+            }
+            if (e < 0 && lim == hi) e = hi;
+        }
         int64_t pos[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) pos[c] = s;
-        int64_t len = hi - s;
+        int64_t len = (e >= 0 ? e : hi) - s;
         while (len > 1) {
             const int64_t half = len >> 1;
 #pragma unroll
@@ -170,7 +190,7 @@ internal_kernel(const uint64_t* __restrict__ keys, int64_t n, const int32_t* __r
         b[0] = s;
 #pragma unroll
         for (int c = 1; c < 8; ++c) b[c] = static_cast<int32_t>(pos[c] + (__ldg(keys + pos[c]) < v[c] ? 1 : 0));
-        b[8] = static_cast<int32_t>(pos[0] + (__ldg(keys + pos[0]) < v[0] ? 1 : 0));
+        b[8] = e >= 0 ? static_cast<int32_t>(e) : static_cast<int32_t>(pos[0] + (__ldg(keys + pos[0]) < v[0] ? 1 : 0));
         int nchild = 0;
         for (int c = 0; c < 8; ++c) nchild += b[c + 1] > b[c];
         int ngroups = 0;
@@ -352,8 +372,21 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
     return old;
 }
 
+// Resident blocks the register allocation must allow: the one-launch pass
+// (leaf moments and climb in one thread) at 4 per SM, the climb launch of the
+// two-launch pass at 2 (no spills: each climbing thread's chain of round
+// trips is the critical path there).
 #ifndef NB_UP_MINB
 #define NB_UP_MINB 4
+#endif
+#ifndef NB_UP_CLIMB_MINB
+#define NB_UP_CLIMB_MINB 2
+#endif
+#ifndef NB_UP_LEAVES_MINB
+#define NB_UP_LEAVES_MINB 3
+#endif
+#ifndef NB_UP_SPLIT
+#define NB_UP_SPLIT 1
 #endif
 #ifndef NB_UP_ONEPASS
 #define NB_UP_ONEPASS 1
@@ -361,11 +394,193 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
 #ifndef NB_UP_ONEPASS_CLIMB
 #define NB_UP_ONEPASS_CLIMB 1
 #endif
-#if NB_UP_MINB > 0
+// Moments of leaf n (bodies [first, first + cnt)), stored.
+__device__ __forceinline__ void leaf_moments(const Bodies& bd, const uint64_t* __restrict__ keys,
+                                             const int32_t* __restrict__ sysid, const double4* __restrict__ cubes,
+                                             int base, const Params& P, Tree& t, bool accurate, int64_t n, int first,
+                                             int cnt) {
+    const int lvl = t.level[n];
+    // an empty leaf can only be the root of an empty system (node id = system)
+    const int sys = sysid ? (cnt > 0 ? sysid[first] : static_cast<int>(n)) : 0;
+    const double4 cube = cubes[sys];
+    const double half = ldexp(cube.w, -lvl);
+    Mom a{};
+    double rcrit = 0.0;
+    if (!accurate) {
+        if (cnt == 1) {
+            a.m = bd.m[first]; a.cx = bd.x[first]; a.cy = bd.y[first]; a.cz = bd.z[first];
+        } else if (cnt > 1) {
+            a = combine_ref(cnt, half, [&](int k) {
+                return make_double4(bd.x[first + k], bd.y[first + k], bd.z[first + k], bd.m[first + k]);
+            });
+        }
+    } else if (NB_UP_ONEPASS) {
+        // one pass over the leaf's bodies: mass, first and second moments
+        // about its first body (all of cell size, so no cancellation),
+        // then shifted to the centre of mass
+        const uint64_t key = cnt > 0 ? keys[first] : 0ull;
+        const double x0 = cnt > 0 ? bd.x[first] : 0.0, y0 = cnt > 0 ? bd.y[first] : 0.0,
+                     z0 = cnt > 0 ? bd.z[first] : 0.0;
+        double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+        for (int j = first; j < first + cnt; ++j) {
+            const double mj = bd.m[j];
+            const double dx = bd.x[j] - x0, dy = bd.y[j] - y0, dz = bd.z[j] - z0;
+            const double mx = mj * dx, my = mj * dy, mz = mj * dz;
+            m += mj; sx += mx; sy += my; sz += mz;
+            sxx += mx * dx; syy += my * dy; szz += mz * dz;
+            sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+        }
+        double cx, cy, cz;
+        if (m > 0) {
+            const double ox = sx / m, oy = sy / m, oz = sz / m;
+            cx = x0 + ox; cy = y0 + oy; cz = z0 + oz;
+            // second moments about the centre of mass
+            const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
+            const double tr = qxx + qyy + qzz;
+            a.q[0] = 3.0 * qxx - tr; a.q[1] = 3.0 * qyy - tr; a.q[2] = 3.0 * qzz - tr;
+            a.q[3] = 3.0 * (sxy - sx * oy); a.q[4] = 3.0 * (sxz - sx * oz); a.q[5] = 3.0 * (syz - sy * oz);
+        } else {
+            const double3 g = cell_centre(key, lvl, cube, base);
+            cx = g.x; cy = g.y; cz = g.z;
+        }
+        a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
+        rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
+    } else {
+        double m = 0, cx = 0, cy = 0, cz = 0;
+        for (int j = first; j < first + cnt; ++j) {
+            const double mj = bd.m[j];
+            m += mj; cx += mj * bd.x[j]; cy += mj * bd.y[j]; cz += mj * bd.z[j];
+        }
+        const uint64_t key = cnt > 0 ? keys[first] : 0ull;
+        if (m > 0) { cx /= m; cy /= m; cz /= m; }
+        else { const double3 g = cell_centre(key, lvl, cube, base); cx = g.x; cy = g.y; cz = g.z; }
+        for (int j = first; j < first + cnt; ++j) {
+            const double rx = bd.x[j] - cx, ry = bd.y[j] - cy, rz = bd.z[j] - cz;
+            const double r2 = rx * rx + ry * ry + rz * rz;
+            const double mj = bd.m[j];
+            a.q[0] += mj * (3.0 * rx * rx - r2); a.q[1] += mj * (3.0 * ry * ry - r2);
+            a.q[2] += mj * (3.0 * rz * rz - r2); a.q[3] += mj * (3.0 * rx * ry);
+            a.q[4] += mj * (3.0 * rx * rz);      a.q[5] += mj * (3.0 * ry * rz);
+        }
+        a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
+        rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
+    }
+    store_moments(t, static_cast<int>(n), a, half, rcrit, P.G, accurate);
+}
+
+// Moments of internal node rec.x from its children rec.y .. rec.y + nchild
+// (all of them final), stored.
+__device__ __forceinline__ void combine_children(const uint64_t* __restrict__ keys, const int32_t* __restrict__ sysid,
+                                                 const double4* __restrict__ cubes, int base, const Params& P, Tree& t,
+                                                 bool accurate, const int4 rec) {
+    const int nid = rec.x;
+    const int2 plk = make_int2(rec.y, rec.z & 0xff);
+    const int pl = rec.z >> 8;
+    const int ps = rec.w;
+    const double4 pcube = cubes[sysid ? sysid[ps] : 0];
+    const double phalf = ldexp(pcube.w, -pl);
+    Mom p{};
+    double prc = 0.0;
+    if (!accurate) {
+        p = combine_ref(plk.y, phalf, [&](int k) { return ldcg4(t.com + plk.x + k); });
+    } else if (NB_UP_ONEPASS_CLIMB) {
+        // one pass over the children: mass, first and second moments of
+        // their centres of mass about the first child's, their own
+        // quadrupoles; then shifted to the parent's centre of mass
+        // (parallel axes)
+        const double4 c0 = ldcg4(t.com + plk.x);
+        double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
+        double qs[6] = {0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < plk.y; ++k) {
+            const double4 c = ldcg4(t.com + plk.x + k);
+            const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
+            const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
+            const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
+            m += c.w; sx += mx; sy += my; sz += mz;
+            sxx += mx * dx; syy += my * dy; szz += mz * dz;
+            sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) qs[f] += __ldcg(cq + f);
+        }
+        const uint64_t key = keys[ps];
+        double cx, cy, cz;
+        if (m > 0) {
+            const double ox = sx / m, oy = sy / m, oz = sz / m;
+            cx = c0.x + ox; cy = c0.y + oy; cz = c0.z + oz;
+            const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
+            const double tr = qxx + qyy + qzz;
+            p.q[0] = qs[0] + (3.0 * qxx - tr); p.q[1] = qs[1] + (3.0 * qyy - tr);
+            p.q[2] = qs[2] + (3.0 * qzz - tr); p.q[3] = qs[3] + 3.0 * (sxy - sx * oy);
+            p.q[4] = qs[4] + 3.0 * (sxz - sx * oz); p.q[5] = qs[5] + 3.0 * (syz - sy * oz);
+        } else {
+            const double3 g = cell_centre(key, pl, pcube, base);
+            cx = g.x; cy = g.y; cz = g.z;
+            for (int f = 0; f < 6; ++f) p.q[f] = qs[f];
+        }
+        p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
+        prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
+    } else {
+        double m = 0, cx = 0, cy = 0, cz = 0;
+        for (int k = 0; k < plk.y; ++k) {
+            const double4 c = ldcg4(t.com + plk.x + k);
+            m += c.w; cx += c.w * c.x; cy += c.w * c.y; cz += c.w * c.z;
+        }
+        const uint64_t key = keys[ps];
+        if (m > 0) { cx /= m; cy /= m; cz /= m; }
+        else { const double3 g = cell_centre(key, pl, pcube, base); cx = g.x; cy = g.y; cz = g.z; }
+        for (int k = 0; k < plk.y; ++k) {
+            const double4 c = ldcg4(t.com + plk.x + k);
+            const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
+            const double rx = c.x - cx, ry = c.y - cy, rz = c.z - cz;
+            const double r2 = rx * rx + ry * ry + rz * rz;
+            const double mk = c.w;
+            p.q[0] += __ldcg(cq + 0) + mk * (3.0 * rx * rx - r2);
+            p.q[1] += __ldcg(cq + 1) + mk * (3.0 * ry * ry - r2);
+            p.q[2] += __ldcg(cq + 2) + mk * (3.0 * rz * rz - r2);
+            p.q[3] += __ldcg(cq + 3) + mk * (3.0 * rx * ry);
+            p.q[4] += __ldcg(cq + 4) + mk * (3.0 * rx * rz);
+            p.q[5] += __ldcg(cq + 5) + mk * (3.0 * ry * rz);
+        }
+        p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
+        prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
+    }
+    store_moments(t, nid, p, phalf, prc, P.G, accurate);
+}
+
+// Validated climb record of internal id q (nullopt-style: ok = false on a bad record).
+__device__ __forceinline__ bool climb_record(const Tree& t, int64_t nodes, int q, int4* rec, int* err) {
+    *rec = __ldg(t.climb + q);
+    const int nc = rec->z & 0xff;
+    if (rec->x < 0 || rec->x >= nodes || nc < 1 || nc > 8 || rec->y < 0 || static_cast<int64_t>(rec->y) + nc > nodes) {
+        raise_error(err, kErrIndex);
+        return false;
+    }
+    return true;
+}
+
+// From internal id q upward: arrive at each parent; the last child's thread
+// combines the parent's children and goes on.
+__device__ __forceinline__ void climb_from(int q, const uint64_t* __restrict__ keys, const int32_t* __restrict__ sysid,
+                                          const double4* __restrict__ cubes, int base, const Params& P, Tree& t,
+                                          bool accurate, int64_t nodes, int64_t ninternal, int* err) {
+    while (q >= 0) {
+        if (q >= ninternal) { raise_error(err, kErrIndex); break; }
+        // the parent's record (written by the child-search pass) and the
+        // arrival both need only q: their round trips overlap
+        int4 rec;
+        const bool ok = climb_record(t, nodes, q, &rec, err);
+        // release this child's moments / acquire the siblings' ones
+        const int old = arrive_acq_rel(t.counter + q);
+        if (!ok || old != (rec.z & 0xff) - 1) break;
+        t.counter[q] = 0;                      // re-armed for the next build
+        const int next_q = t.parent[rec.x];   // in flight beside the children's loads
+        combine_children(keys, sysid, cubes, base, P, t, accurate, rec);
+        q = next_q;
+    }
+}
+
+// One launch: one thread per leaf computes its moments and climbs.
 __global__ void __launch_bounds__(256, NB_UP_MINB)
-#else
-__global__ void
-#endif
 upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                               const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P,
                               Tree t, int* err) {
@@ -377,169 +592,66 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
          n += (int64_t)gridDim.x * blockDim.x) {
         const int2 lk = t.link[n];
         if (lk.y > 0) continue;                    // internal: filled by a climbing thread
-        const int first = lk.x, cnt = -lk.y;
-        if (first < 0 || static_cast<int64_t>(first) + cnt > nbodies) { raise_error(err, kErrIndex); continue; }
-        const int lvl = t.level[n];
-        // an empty leaf can only be the root of an empty system (node id = system)
-        const int sys = sysid ? (cnt > 0 ? sysid[first] : static_cast<int>(n)) : 0;
-        const double4 cube = cubes[sys];
-        const double half = ldexp(cube.w, -lvl);
-        Mom a{};
-        double rcrit = 0.0;
-        if (!accurate) {
-            if (cnt == 1) {
-                a.m = bd.m[first]; a.cx = bd.x[first]; a.cy = bd.y[first]; a.cz = bd.z[first];
-            } else if (cnt > 1) {
-                a = combine_ref(cnt, half, [&](int k) {
-                    return make_double4(bd.x[first + k], bd.y[first + k], bd.z[first + k], bd.m[first + k]);
-                });
-            }
-        } else if (NB_UP_ONEPASS) {
-            // one pass over the leaf's bodies: mass, first and second moments
-            // about its first body (all of cell size, so no cancellation),
-            // then shifted to the centre of mass
-            const uint64_t key = cnt > 0 ? keys[first] : 0ull;
-            const double x0 = cnt > 0 ? bd.x[first] : 0.0, y0 = cnt > 0 ? bd.y[first] : 0.0,
-                         z0 = cnt > 0 ? bd.z[first] : 0.0;
-            double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-            for (int j = first; j < first + cnt; ++j) {
-                const double mj = bd.m[j];
-                const double dx = bd.x[j] - x0, dy = bd.y[j] - y0, dz = bd.z[j] - z0;
-                const double mx = mj * dx, my = mj * dy, mz = mj * dz;
-                m += mj; sx += mx; sy += my; sz += mz;
-                sxx += mx * dx; syy += my * dy; szz += mz * dz;
-                sxy += mx * dy; sxz += mx * dz; syz += my * dz;
-            }
-            double cx, cy, cz;
-            if (m > 0) {
-                const double ox = sx / m, oy = sy / m, oz = sz / m;
-                cx = x0 + ox; cy = y0 + oy; cz = z0 + oz;
-                // second moments about the centre of mass
-                const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
-                const double tr = qxx + qyy + qzz;
-                a.q[0] = 3.0 * qxx - tr; a.q[1] = 3.0 * qyy - tr; a.q[2] = 3.0 * qzz - tr;
-                a.q[3] = 3.0 * (sxy - sx * oy); a.q[4] = 3.0 * (sxz - sx * oz); a.q[5] = 3.0 * (syz - sy * oz);
-            } else {
-                const double3 g = cell_centre(key, lvl, cube, base);
-                cx = g.x; cy = g.y; cz = g.z;
-            }
-            a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
-            rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
-        } else {
-            double m = 0, cx = 0, cy = 0, cz = 0;
-            for (int j = first; j < first + cnt; ++j) {
-                const double mj = bd.m[j];
-                m += mj; cx += mj * bd.x[j]; cy += mj * bd.y[j]; cz += mj * bd.z[j];
-            }
-            const uint64_t key = cnt > 0 ? keys[first] : 0ull;
-            if (m > 0) { cx /= m; cy /= m; cz /= m; }
-            else { const double3 g = cell_centre(key, lvl, cube, base); cx = g.x; cy = g.y; cz = g.z; }
-            for (int j = first; j < first + cnt; ++j) {
-                const double rx = bd.x[j] - cx, ry = bd.y[j] - cy, rz = bd.z[j] - cz;
-                const double r2 = rx * rx + ry * ry + rz * rz;
-                const double mj = bd.m[j];
-                a.q[0] += mj * (3.0 * rx * rx - r2); a.q[1] += mj * (3.0 * ry * ry - r2);
-                a.q[2] += mj * (3.0 * rz * rz - r2); a.q[3] += mj * (3.0 * rx * ry);
-                a.q[4] += mj * (3.0 * rx * rz);      a.q[5] += mj * (3.0 * ry * rz);
-            }
-            a.m = m; a.cx = cx; a.cy = cy; a.cz = cz;
-            rcrit = rcrit_of(a, key, lvl, cube, base, half, P.theta);
-        }
-        store_moments(t, static_cast<int>(n), a, half, rcrit, P.G, accurate);
-        // climb
-        int q = t.parent[n];
-        while (q >= 0) {
-            if (q >= ninternal) { raise_error(err, kErrIndex); break; }
-            // the parent's record (written by the child-search pass) and the
-            // arrival both need only q: their round trips overlap
-            const int4 rec = __ldg(t.climb + q);
-            // release this child's moments / acquire the siblings' ones
-            const int old = arrive_acq_rel(t.counter + q);
-            const int nid = rec.x;
-            const int2 plk = make_int2(rec.y, rec.z & 0xff);
-            if (nid < 0 || nid >= nodes || plk.y < 1 || plk.y > 8 || plk.x < 0 ||
-                static_cast<int64_t>(plk.x) + plk.y > nodes) {
-                raise_error(err, kErrIndex);
-                break;
-            }
-            if (old != plk.y - 1) break;
-            t.counter[q] = 0;                      // re-armed for the next build
-            const int next_q = t.parent[nid];     // in flight beside the children's loads
-            const int pl = rec.z >> 8;
-            const int ps = rec.w;
-            const double4 pcube = cubes[sysid ? sysid[ps] : 0];
-            const double phalf = ldexp(pcube.w, -pl);
-            Mom p{};
-            double prc = 0.0;
-            if (!accurate) {
-                p = combine_ref(plk.y, phalf, [&](int k) { return ldcg4(t.com + plk.x + k); });
-            } else if (NB_UP_ONEPASS_CLIMB) {
-                // one pass over the children: mass, first and second moments of
-                // their centres of mass about the first child's, their own
-                // quadrupoles; then shifted to the parent's centre of mass
-                // (parallel axes)
-                const double4 c0 = ldcg4(t.com + plk.x);
-                double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
-                double qs[6] = {0, 0, 0, 0, 0, 0};
-                for (int k = 0; k < plk.y; ++k) {
-                    const double4 c = ldcg4(t.com + plk.x + k);
-                    const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
-                    const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
-                    const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
-                    m += c.w; sx += mx; sy += my; sz += mz;
-                    sxx += mx * dx; syy += my * dy; szz += mz * dz;
-                    sxy += mx * dy; sxz += mx * dz; syz += my * dz;
-#pragma unroll
-                    for (int f = 0; f < 6; ++f) qs[f] += __ldcg(cq + f);
-                }
-                const uint64_t key = keys[ps];
-                double cx, cy, cz;
-                if (m > 0) {
-                    const double ox = sx / m, oy = sy / m, oz = sz / m;
-                    cx = c0.x + ox; cy = c0.y + oy; cz = c0.z + oz;
-                    const double qxx = sxx - sx * ox, qyy = syy - sy * oy, qzz = szz - sz * oz;
-                    const double tr = qxx + qyy + qzz;
-                    p.q[0] = qs[0] + (3.0 * qxx - tr); p.q[1] = qs[1] + (3.0 * qyy - tr);
-                    p.q[2] = qs[2] + (3.0 * qzz - tr); p.q[3] = qs[3] + 3.0 * (sxy - sx * oy);
-                    p.q[4] = qs[4] + 3.0 * (sxz - sx * oz); p.q[5] = qs[5] + 3.0 * (syz - sy * oz);
-                } else {
-                    const double3 g = cell_centre(key, pl, pcube, base);
-                    cx = g.x; cy = g.y; cz = g.z;
-                    for (int f = 0; f < 6; ++f) p.q[f] = qs[f];
-                }
-                p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
-                prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
-            } else {
-                double m = 0, cx = 0, cy = 0, cz = 0;
-                for (int k = 0; k < plk.y; ++k) {
-                    const double4 c = ldcg4(t.com + plk.x + k);
-                    m += c.w; cx += c.w * c.x; cy += c.w * c.y; cz += c.w * c.z;
-                }
-                const uint64_t key = keys[ps];
-                if (m > 0) { cx /= m; cy /= m; cz /= m; }
-                else { const double3 g = cell_centre(key, pl, pcube, base); cx = g.x; cy = g.y; cz = g.z; }
-                for (int k = 0; k < plk.y; ++k) {
-                    const double4 c = ldcg4(t.com + plk.x + k);
-                    const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
-                    const double rx = c.x - cx, ry = c.y - cy, rz = c.z - cz;
-                    const double r2 = rx * rx + ry * ry + rz * rz;
-                    const double mk = c.w;
-                    p.q[0] += __ldcg(cq + 0) + mk * (3.0 * rx * rx - r2);
-                    p.q[1] += __ldcg(cq + 1) + mk * (3.0 * ry * ry - r2);
-                    p.q[2] += __ldcg(cq + 2) + mk * (3.0 * rz * rz - r2);
-                    p.q[3] += __ldcg(cq + 3) + mk * (3.0 * rx * ry);
-                    p.q[4] += __ldcg(cq + 4) + mk * (3.0 * rx * rz);
-                    p.q[5] += __ldcg(cq + 5) + mk * (3.0 * ry * rz);
-                }
-                p.m = m; p.cx = cx; p.cy = cy; p.cz = cz;
-                prc = rcrit_of(p, key, pl, pcube, base, phalf, P.theta);
-            }
-            store_moments(t, nid, p, phalf, prc, P.G, accurate);
-            q = next_q;
+        if (lk.x < 0 || static_cast<int64_t>(lk.x) - lk.y > nbodies) { raise_error(err, kErrIndex); continue; }
+        leaf_moments(bd, keys, sysid, cubes, base, P, t, accurate, n, lk.x, -lk.y);
+        climb_from(t.parent[n], keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
+    }
+}
+
+// Two launches.  Leaves: one thread per leaf computes its moments and counts
+// itself in at its parent (a plain atomic: the climb launch that reads the
+// moments comes after this one); a parent all of whose children are leaves
+// is complete when its last leaf arrives, and goes on the ready list.
+__global__ void __launch_bounds__(256, NB_UP_LEAVES_MINB)
+upward_leaves_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
+                     const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P, Tree t,
+                     int* err) {
+    if (*err & kErrAbort) return;
+    const bool accurate = P.physics == NEXT_PHYSICS_ACCURATE;
+    const int64_t nodes = t.counts[1];
+    const int64_t ninternal = t.counts[0];
+    for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes;
+         n += (int64_t)gridDim.x * blockDim.x) {
+        const int2 lk = t.link[n];
+        if (lk.y > 0) continue;
+        if (lk.x < 0 || static_cast<int64_t>(lk.x) - lk.y > nbodies) { raise_error(err, kErrIndex); continue; }
+        leaf_moments(bd, keys, sysid, cubes, base, P, t, accurate, n, lk.x, -lk.y);
+        const int q = t.parent[n];
+        if (q < 0) continue;
+        if (q >= ninternal) { raise_error(err, kErrIndex); continue; }
+        int4 rec;
+        if (!climb_record(t, nodes, q, &rec, err)) continue;
+        if (atomicAdd(t.counter + q, 1) == (rec.z & 0xff) - 1) {
+            t.counter[q] = 0;
+            const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(t.counts + 4), 1ull);
+            if (slot < static_cast<unsigned long long>(t.cap_int)) t.ready[slot] = q;
+            else raise_error(err, kErrIndex);
         }
     }
 }
 
+// Climb: one thread per ready parent combines its (leaf) children and
+// climbs on as in the one-launch form; the parents' arrival counters already
+// hold their leaf children.
+__global__ void __launch_bounds__(256, NB_UP_CLIMB_MINB)
+upward_climb_kernel(const uint64_t* __restrict__ keys, const int32_t* __restrict__ sysid,
+                    const double4* __restrict__ cubes, int base, Params P, Tree t, int* err) {
+    if (*err & kErrAbort) return;
+    const bool accurate = P.physics == NEXT_PHYSICS_ACCURATE;
+    const int64_t nodes = t.counts[1];
+    const int64_t ninternal = t.counts[0];
+    const int64_t nready = t.counts[4] < t.cap_int ? t.counts[4] : t.cap_int;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nready;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int q = t.ready[i];
+        if (q < 0 || q >= ninternal) { raise_error(err, kErrIndex); continue; }
+        int4 rec;
+        if (!climb_record(t, nodes, q, &rec, err)) continue;
+        const int next_q = t.parent[rec.x];
+        combine_children(keys, sysid, cubes, base, P, t, accurate, rec);
+        climb_from(next_q, keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
+    }
+}
 }  // namespace
 
 cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const int32_t* sysid,
@@ -551,7 +663,7 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
     const int group_cap = P.group_cap < leaf_cap ? leaf_cap : P.group_cap;
     const int32_t* sid = sys.n > 1 ? sysid : nullptr;
     const int64_t* offs = sys.n > 1 ? d_offsets : nullptr;
-    cudaError_t e0 = cudaMemsetAsync(t.counts + 3, 0, sizeof(int64_t), st);
+    cudaError_t e0 = cudaMemsetAsync(t.counts + 3, 0, 2 * sizeof(int64_t), st);
     if (e0 != cudaSuccess) return e0;
     if (n > 0) {
         dlev_kernel<<<blocks, threads, 0, st>>>(keys, n, sys.base, sys.levels, t.dlev);
@@ -579,8 +691,16 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
         keys, t.dlev, t.nint, sid, sys.n, sys.levels, leaf_cap, group_cap, t, err);
     const unsigned ublocks = static_cast<unsigned>((t.cap_node + threads - 1) / threads);
     Params Pu = P;
-    upward_kernel<<<ublocks < 8192u ? ublocks : 8192u, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu,
-                                                                         t, err);
+    const unsigned ugrid = ublocks < 8192u ? ublocks : 8192u;
+    if (NB_UP_SPLIT) {
+        upward_leaves_kernel<<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
+        const unsigned rblocks = static_cast<unsigned>((t.cap_int + threads - 1) / threads);
+        upward_climb_kernel<<<rblocks < 8192u ? (rblocks ? rblocks : 1u) : 8192u, threads, 0, st>>>(
+            keys, sid, sys.cube, sys.base, Pu, t, err);
+        count_launches(1);
+    } else {
+        upward_kernel<<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
+    }
     count_launches(n > 0 ? 9 : 5);
     return cudaGetLastError();
 }
