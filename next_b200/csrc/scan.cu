@@ -10,6 +10,9 @@ namespace nb {
 
 namespace {
 
+#ifndef NB_SCAN_VEC
+#define NB_SCAN_VEC 1
+#endif
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -89,24 +92,45 @@ tile_scan_kernel(const T* __restrict__ in, T* __restrict__ out, int64_t n, const
     const int64_t cnt = scan_count<T>(n, count_dev);
     const int64_t base = static_cast<int64_t>(blockIdx.x) * kScanTile;
     if (base > cnt) return;
-    // blocked layout: thread t owns items base + t*kScanItems .. +kScanItems
+    // blocked layout: thread t owns items base + t*kScanItems .. +kScanItems,
+    // moved as 16-byte vectors when all of them lie below the count
+    constexpr int kVec = kScanItems * static_cast<int>(sizeof(T)) / 16;
+    const int64_t first = base + static_cast<int64_t>(threadIdx.x) * kScanItems;
+    const bool whole = NB_SCAN_VEC && first + kScanItems <= cnt;
     T v[kScanItems];
     T s = 0;
-    for (int k = 0; k < kScanItems; ++k) {
-        const int64_t i = base + threadIdx.x * kScanItems + k;
-        v[k] = i < cnt ? in[i] : T(0);
-        s += v[k];
+    if (whole) {
+        const uint4* src = reinterpret_cast<const uint4*>(in + first);
+#pragma unroll
+        for (int q = 0; q < kVec; ++q) reinterpret_cast<uint4*>(v)[q] = src[q];
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) s += v[k];
+    } else {
+        for (int k = 0; k < kScanItems; ++k) {
+            const int64_t i = first + k;
+            v[k] = i < cnt ? in[i] : T(0);
+            s += v[k];
+        }
     }
     T total;
     T run = block_exclusive_scan<T>(s, &total) + sums[blockIdx.x];
-    for (int k = 0; k < kScanItems; ++k) {
-        const int64_t i = base + threadIdx.x * kScanItems + k;
-        if (i < cnt) out[i] = run;
-        if (i == cnt) {
-            out[i] = run;
-            if (total_dev) *total_dev = static_cast<int64_t>(run);
+    if (whole) {
+        T o[kScanItems];
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) { o[k] = run; run += v[k]; }
+        uint4* dst = reinterpret_cast<uint4*>(out + first);
+#pragma unroll
+        for (int q = 0; q < kVec; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
+    } else {                                        // also the owner of out[cnt]
+        for (int k = 0; k < kScanItems; ++k) {
+            const int64_t i = first + k;
+            if (i < cnt) out[i] = run;
+            if (i == cnt) {
+                out[i] = run;
+                if (total_dev) *total_dev = static_cast<int64_t>(run);
+            }
+            run += v[k];
         }
-        run += v[k];
     }
 }
 
