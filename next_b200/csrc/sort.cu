@@ -32,17 +32,7 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr int kSpinLimit = 1 << 20;
-// Earlier tiles whose status one look-back step reads: 8 in general; sorts
-// of at most NB_SORT_SMALL_N pairs, whose tiles all run at once, wait on the
-// length of the look-back chain (tiles / window round trips) and read wider
-// windows.
-constexpr int kLookWindow = 8;
-#ifndef NB_SORT_SMALL_N
-#define NB_SORT_SMALL_N 0
-#endif
-#ifndef NB_SORT_SMALL_WINDOW
-#define NB_SORT_SMALL_WINDOW 32
-#endif
+constexpr int kLookWindow = 8;   // earlier tiles whose status one look-back step reads
 
 // Digit mask of pass p for keys of key_bits significant bits: bits at and
 // above key_bits take no part in the ordering.
@@ -139,7 +129,6 @@ __device__ __forceinline__ void load_tile(const uint64_t* __restrict__ keys_in, 
 // tile's pairs sit ranked in shared memory, the block takes its next ticket
 // and loads that tile into the registers the ranking has freed, so the load
 // runs while this tile waits on its look-back and writes itself out.
-template <int W>
 __global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
@@ -185,9 +174,9 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         volatile uint32_t* vstat = status;
         if (tile == 0) vstat[d] = kFlagInc | count;
         else vstat[static_cast<int64_t>(tile) * kRadix + d] = kFlagAgg | count;
-        uint32_t win[W];
+        uint32_t win[kLookWindow];
 #pragma unroll
-        for (int j = 0; j < W; ++j)
+        for (int j = 0; j < kLookWindow; ++j)
             win[j] = tile - 1 - j >= 0 ? vstat[static_cast<int64_t>(tile - 1 - j) * kRadix + d]
                                        : static_cast<uint32_t>(kFlagInc);
         // Exclusive scan of the tile counts over digits: warp scans + warp totals.
@@ -234,7 +223,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
             bool done = false, timed_out = false;
             while (!done) {
 #pragma unroll
-                for (int j = 0; j < W; ++j) {
+                for (int j = 0; j < kLookWindow; ++j) {
                     if (done) break;
                     uint32_t v = win[j];
                     int spins = 0;
@@ -246,9 +235,9 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
                     done = (v & kFlagInc) || timed_out || pred - j == 0;
                 }
                 if (done) break;
-                pred -= W;
+                pred -= kLookWindow;
 #pragma unroll
-                for (int j = 0; j < W; ++j)
+                for (int j = 0; j < kLookWindow; ++j)
                     win[j] = pred - j >= 0 ? vstat[static_cast<int64_t>(pred - j) * kRadix + d]
                                            : static_cast<uint32_t>(kFlagInc);
             }
@@ -297,7 +286,7 @@ static unsigned onesweep_grid(int64_t tiles) {
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<kLookWindow>, kThreads, sizeof(SortSmem)) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kThreads, sizeof(SortSmem)) !=
             cudaSuccess ||
         per_sm < 1 || sms < 1)
         return static_cast<unsigned>(tiles);
@@ -306,24 +295,8 @@ static unsigned onesweep_grid(int64_t tiles) {
 }
 
 cudaError_t sort_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(onesweep_kernel<kLookWindow>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(SortSmem)));
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(onesweep_kernel<NB_SORT_SMALL_WINDOW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sizeof(SortSmem)));
-    return e;
-}
-
-// One onesweep pass with the look-back window for this sort's size.
-static void launch_onesweep(int64_t tiles, cudaStream_t st, const uint64_t* ki, const uint32_t* vi, uint64_t* ko,
-                            uint32_t* vo, int64_t n, int shift, uint32_t dmask, const uint32_t* offs, uint32_t* status,
-                            unsigned int* ticket, int* err) {
-    if (n <= NB_SORT_SMALL_N)
-        onesweep_kernel<NB_SORT_SMALL_WINDOW><<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
-            ki, vi, ko, vo, n, shift, dmask, offs, status, ticket, err);
-    else
-        onesweep_kernel<kLookWindow><<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
-            ki, vi, ko, vo, n, shift, dmask, offs, status, ticket, err);
+    return cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(sizeof(SortSmem)));
 }
 
 // Sorts (keys, vals) of length n using (alt_keys, alt_vals) as the other
@@ -350,8 +323,9 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
     uint64_t* src_k = keys; uint32_t* src_v = vals;
     uint64_t* dst_k = alt_keys; uint32_t* dst_v = alt_vals;
     for (int p = 0; p < passes; ++p) {
-        launch_onesweep(tiles, st, src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
-                        status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
+            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
+            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         uint64_t* tk = src_k; src_k = dst_k; dst_k = tk;
         uint32_t* tv = src_v; src_v = dst_v; dst_v = tv;
     }
@@ -397,8 +371,9 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
         const bool to_out = ((passes - 1 - p) & 1) == 0;
         uint64_t* dst_k = to_out ? keys_out : alt_keys;
         uint32_t* dst_v = to_out ? vals_out : alt_vals;
-        launch_onesweep(tiles, st, src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
-                        status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
+            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
+            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
         src_k = dst_k;
         src_v = dst_v;
     }
