@@ -385,6 +385,11 @@ __device__ __forceinline__ int arrive_acq_rel(int32_t* counter) {
 #ifndef NB_UP_LEAVES_MINB
 #define NB_UP_LEAVES_MINB 3
 #endif
+// Children whose records a combining thread loads together (2: no spills
+// at the climb launch's register cap; 4 and 8 spill and run slower).
+#ifndef NB_UP_CHUNK
+#define NB_UP_CHUNK 2
+#endif
 #ifndef NB_UP_SPLIT
 #define NB_UP_SPLIT 1
 #endif
@@ -491,16 +496,46 @@ __device__ __forceinline__ void combine_children(const uint64_t* __restrict__ ke
         const double4 c0 = ldcg4(t.com + plk.x);
         double m = 0, sx = 0, sy = 0, sz = 0, sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0;
         double qs[6] = {0, 0, 0, 0, 0, 0};
-        for (int k = 0; k < plk.y; ++k) {
-            const double4 c = ldcg4(t.com + plk.x + k);
-            const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
-            const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
-            const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
-            m += c.w; sx += mx; sy += my; sz += mz;
-            sxx += mx * dx; syy += my * dy; szz += mz * dz;
-            sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+        if (NB_UP_CHUNK > 1) {
+            // the children's records in chunks whose loads are all in flight
+            // together, summed in octant order as below
+            for (int k0 = 0; k0 < plk.y; k0 += NB_UP_CHUNK) {
+                double4 cc[NB_UP_CHUNK];
+                double2 cq[NB_UP_CHUNK][3];
 #pragma unroll
-            for (int f = 0; f < 6; ++f) qs[f] += __ldcg(cq + f);
+                for (int u = 0; u < NB_UP_CHUNK; ++u) {
+                    if (k0 + u < plk.y) {
+                        cc[u] = ldcg4(t.com + plk.x + k0 + u);
+                        const double2* q2 = reinterpret_cast<const double2*>(t.quad64 + 8 * static_cast<int64_t>(plk.x + k0 + u));
+#pragma unroll
+                        for (int f = 0; f < 3; ++f) cq[u][f] = __ldcg(q2 + f);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < NB_UP_CHUNK; ++u) {
+                    if (k0 + u >= plk.y) break;
+                    const double4 c = cc[u];
+                    const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
+                    const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
+                    m += c.w; sx += mx; sy += my; sz += mz;
+                    sxx += mx * dx; syy += my * dy; szz += mz * dz;
+                    sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+#pragma unroll
+                    for (int f = 0; f < 3; ++f) { qs[2 * f] += cq[u][f].x; qs[2 * f + 1] += cq[u][f].y; }
+                }
+            }
+        } else {
+            for (int k = 0; k < plk.y; ++k) {
+                const double4 c = ldcg4(t.com + plk.x + k);
+                const double* cq = t.quad64 + 8 * static_cast<int64_t>(plk.x + k);
+                const double dx = c.x - c0.x, dy = c.y - c0.y, dz = c.z - c0.z;
+                const double mx = c.w * dx, my = c.w * dy, mz = c.w * dz;
+                m += c.w; sx += mx; sy += my; sz += mz;
+                sxx += mx * dx; syy += my * dy; szz += mz * dz;
+                sxy += mx * dy; sxz += mx * dz; syz += my * dz;
+#pragma unroll
+                for (int f = 0; f < 6; ++f) qs[f] += __ldcg(cq + f);
+            }
         }
         const uint64_t key = keys[ps];
         double cx, cy, cz;
@@ -559,20 +594,27 @@ __device__ __forceinline__ bool climb_record(const Tree& t, int64_t nodes, int q
 }
 
 // From internal id q upward: arrive at each parent; the last child's thread
-// combines the parent's children and goes on.
-__device__ __forceinline__ void climb_from(int q, const uint64_t* __restrict__ keys, const int32_t* __restrict__ sysid,
-                                          const double4* __restrict__ cubes, int base, const Params& P, Tree& t,
-                                          bool accurate, int64_t nodes, int64_t ninternal, int* err) {
+// combines the parent's children and goes on.  complete: q's children are
+// all final already (no arrival at q itself).
+__device__ __forceinline__ void climb_from(int q, bool complete, const uint64_t* __restrict__ keys,
+                                          const int32_t* __restrict__ sysid, const double4* __restrict__ cubes,
+                                          int base, const Params& P, Tree& t, bool accurate, int64_t nodes,
+                                          int64_t ninternal, int* err) {
     while (q >= 0) {
         if (q >= ninternal) { raise_error(err, kErrIndex); break; }
         // the parent's record (written by the child-search pass) and the
         // arrival both need only q: their round trips overlap
         int4 rec;
         const bool ok = climb_record(t, nodes, q, &rec, err);
-        // release this child's moments / acquire the siblings' ones
-        const int old = arrive_acq_rel(t.counter + q);
-        if (!ok || old != (rec.z & 0xff) - 1) break;
-        t.counter[q] = 0;                      // re-armed for the next build
+        if (!complete) {
+            // release this child's moments / acquire the siblings' ones
+            const int old = arrive_acq_rel(t.counter + q);
+            if (!ok || old != (rec.z & 0xff) - 1) break;
+            t.counter[q] = 0;                  // re-armed for the next build
+        } else if (!ok) {
+            break;
+        }
+        complete = false;
         const int next_q = t.parent[rec.x];   // in flight beside the children's loads
         combine_children(keys, sysid, cubes, base, P, t, accurate, rec);
         q = next_q;
@@ -594,7 +636,7 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
         if (lk.y > 0) continue;                    // internal: filled by a climbing thread
         if (lk.x < 0 || static_cast<int64_t>(lk.x) - lk.y > nbodies) { raise_error(err, kErrIndex); continue; }
         leaf_moments(bd, keys, sysid, cubes, base, P, t, accurate, n, lk.x, -lk.y);
-        climb_from(t.parent[n], keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
+        climb_from(t.parent[n], false, keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
     }
 }
 
@@ -602,12 +644,13 @@ upward_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
 // itself in at its parent (a plain atomic: the climb launch that reads the
 // moments comes after this one); a parent all of whose children are leaves
 // is complete when its last leaf arrives, and goes on the ready list.
+template <bool ACCURATE>
 __global__ void __launch_bounds__(256, NB_UP_LEAVES_MINB)
 upward_leaves_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ keys,
                      const int32_t* __restrict__ sysid, const double4* __restrict__ cubes, int base, Params P, Tree t,
                      int* err) {
     if (*err & kErrAbort) return;
-    const bool accurate = P.physics == NEXT_PHYSICS_ACCURATE;
+    constexpr bool accurate = ACCURATE;
     const int64_t nodes = t.counts[1];
     const int64_t ninternal = t.counts[0];
     for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nodes;
@@ -633,23 +676,20 @@ upward_leaves_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ ke
 // Climb: one thread per ready parent combines its (leaf) children and
 // climbs on as in the one-launch form; the parents' arrival counters already
 // hold their leaf children.
+template <bool ACCURATE>
 __global__ void __launch_bounds__(256, NB_UP_CLIMB_MINB)
 upward_climb_kernel(const uint64_t* __restrict__ keys, const int32_t* __restrict__ sysid,
                     const double4* __restrict__ cubes, int base, Params P, Tree t, int* err) {
     if (*err & kErrAbort) return;
-    const bool accurate = P.physics == NEXT_PHYSICS_ACCURATE;
+    constexpr bool accurate = ACCURATE;
     const int64_t nodes = t.counts[1];
     const int64_t ninternal = t.counts[0];
     const int64_t nready = t.counts[4] < t.cap_int ? t.counts[4] : t.cap_int;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nready;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int q = t.ready[i];
-        if (q < 0 || q >= ninternal) { raise_error(err, kErrIndex); continue; }
-        int4 rec;
-        if (!climb_record(t, nodes, q, &rec, err)) continue;
-        const int next_q = t.parent[rec.x];
-        combine_children(keys, sysid, cubes, base, P, t, accurate, rec);
-        climb_from(next_q, keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
+        if (q < 0) { raise_error(err, kErrIndex); continue; }
+        climb_from(q, true, keys, sysid, cubes, base, P, t, accurate, nodes, ninternal, err);
     }
 }
 }  // namespace
@@ -693,10 +733,17 @@ cudaError_t build_tree(const uint64_t* keys, int64_t n, const Bodies& bd, const 
     Params Pu = P;
     const unsigned ugrid = ublocks < 8192u ? ublocks : 8192u;
     if (NB_UP_SPLIT) {
-        upward_leaves_kernel<<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
+        const bool acc = P.physics == NEXT_PHYSICS_ACCURATE;
+        if (acc)
+            upward_leaves_kernel<true><<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
+        else
+            upward_leaves_kernel<false><<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
         const unsigned rblocks = static_cast<unsigned>((t.cap_int + threads - 1) / threads);
-        upward_climb_kernel<<<rblocks < 8192u ? (rblocks ? rblocks : 1u) : 8192u, threads, 0, st>>>(
-            keys, sid, sys.cube, sys.base, Pu, t, err);
+        const unsigned rgrid = rblocks < 8192u ? (rblocks ? rblocks : 1u) : 8192u;
+        if (acc)
+            upward_climb_kernel<true><<<rgrid, threads, 0, st>>>(keys, sid, sys.cube, sys.base, Pu, t, err);
+        else
+            upward_climb_kernel<false><<<rgrid, threads, 0, st>>>(keys, sid, sys.cube, sys.base, Pu, t, err);
         count_launches(1);
     } else {
         upward_kernel<<<ugrid, threads, 0, st>>>(bd, n, keys, sid, sys.cube, sys.base, Pu, t, err);
