@@ -18,13 +18,17 @@
 // Child bounds: one thread per internal cell runs the eight lower-bound
 // searches for the cell's end and child starts together.
 //
-// Upward pass: one thread per leaf computes the leaf's moments, then climbs;
-// at each parent an atomic arrival counter elects the last child's thread to
-// combine all children in octant order (deterministic), and that thread
-// climbs on.  One launch, no per-level loop.  With accurate physics a leaf's
-// bodies and a cell's children are each read in one pass (moments about the
-// first one, shifted to the centre of mass by the parallel-axis rule); the
-// reference's physics keeps its own two-pass order for bit-exact moments.
+// Upward pass, two launches and no per-level loop: one thread per leaf
+// computes the leaf's moments and counts itself in at its parent; parents
+// whose children are all leaves are then complete and go on a ready list.
+// The second launch runs one thread per ready parent: it combines the
+// children and climbs, an atomic arrival counter at each parent electing the
+// last child's thread to combine all children in octant order
+// (deterministic) and climb on.  With accurate physics a leaf's bodies and a
+// cell's children are each read in one pass (moments about the first one,
+// shifted to the centre of mass by the parallel-axis rule); the reference's
+// physics keeps its own two-pass order for bit-exact moments.  The one-launch
+// form (each leaf's thread climbing) is kept behind NB_UP_SPLIT=0.
 //
 // Built with -fmad=false: every FP64 + and * rounds separately, so the
 // reference-mode moments repeat src/gravity/octree.h:92-127 bit for bit.
