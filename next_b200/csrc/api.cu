@@ -150,8 +150,9 @@ struct next_handle {
     bool have_bodies = false;
     bool forces_valid = false;
     // octant levels held in the keys: the full 21 by default; the FP32-mixed
-    // walk of accurate physics trims them to the measured tree depth + 3 once
-    // per uploaded state (fewer FP64 key levels, fewer sort passes)
+    // walk of accurate physics trims them to at least the measured tree depth
+    // + 2, filling whole sort digits, once per uploaded state (fewer FP64 key
+    // levels, fewer sort passes)
     int sys_bits = 0;                 // bits of the system number above the octant digits
     int key_bits = 63;                // sorted key bits
     bool depth_decided = false;
@@ -420,6 +421,19 @@ void set_key_levels(next_handle* h, int levels) {
     h->key_bits = base + h->sys_bits;
 }
 
+#ifndef NB_KEY_MARGIN
+#define NB_KEY_MARGIN 2
+#endif
+// Key levels kept once the tree depth is known: at least two below the
+// deepest leaf level, and as many more as fill the 8-bit sort digits those
+// need (whole passes either way, so the extra levels cost nothing): 1 M-body
+// uniform sphere 10 levels (4 passes), 16.7 M-body halo 18 (7 passes).
+int trimmed_levels(const next_handle* h, int64_t deepest) {
+    const int need = h->sys_bits + 3 * (static_cast<int>(deepest) + NB_KEY_MARGIN);
+    const int bits = 8 * ((need + 7) / 8);
+    return (bits - h->sys_bits) / 3;
+}
+
 bool adaptive_depth(const next_handle* h) {
     return group_walk(h) && h->P.physics == NEXT_PHYSICS_ACCURATE;
 }
@@ -439,7 +453,8 @@ int read_device_error(next_handle* h, int* bits) {
     h->depth_seen = h->builds;
     if (*bits == 0 && deepest > 0 && adaptive_depth(h)) {
         if (!h->depth_decided) {
-            if (deepest + 3 < h->sys.levels) set_key_levels(h, static_cast<int>(deepest) + 3);
+            const int keep = trimmed_levels(h, deepest);
+            if (keep < h->sys.levels) set_key_levels(h, keep);
         } else if (deepest >= kDepthOverfull) {
             set_key_levels(h, h->sys.levels + 3);
         }

@@ -586,7 +586,8 @@ __device__ __forceinline__ void combine_children(const uint64_t* __restrict__ ke
     store_moments(t, nid, p, phalf, prc, P.G, accurate);
 }
 
-// Validated climb record of internal id q (nullopt-style: ok = false on a bad record).
+// Climb record of internal id q; false (and the index error raised) when it
+// does not describe a node with 1-8 children inside the node array.
 __device__ __forceinline__ bool climb_record(const Tree& t, int64_t nodes, int q, int4* rec, int* err) {
     *rec = __ldg(t.climb + q);
     const int nc = rec->z & 0xff;

@@ -291,7 +291,8 @@ def test_fp64_group_graph_steps_equal_eager_steps():
 
 def test_mixed_steps_trim_key_depth(oracle):
     """After the first build the FP32-mixed path keeps only the measured tree
-    depth + 3 octant levels in its keys; forces stay as accurate and match a
+    depth + 2 octant levels (or more, filling whole sort digits) in its keys;
+    forces stay as accurate and match a
     full-depth build of the same state (same tree, bodies within a leaf may be
     in another order)."""
     b = ic.plummer(60_000, seed=21)
