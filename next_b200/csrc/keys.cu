@@ -75,11 +75,7 @@ system_cubes_kernel(const double* __restrict__ x, const double* __restrict__ y,
 }
 
 // Bodies per thread (two: more independent descents in flight per thread;
-// 16.7 M-body halo 2.00 -> 1.96 ms build less sort); NB_KEYS_UNROLL runs the
-// descent over a fixed 21 levels with the deeper ones masked (not faster).
-#ifndef NB_KEYS_UNROLL
-#define NB_KEYS_UNROLL 0
-#endif
+// 16.7 M-body halo 2.00 -> 1.96 ms build less sort).
 #ifndef NB_KEYS_PER_THREAD
 #define NB_KEYS_PER_THREAD 2
 #endif
@@ -98,34 +94,16 @@ keys_kernel(const double* __restrict__ x, const double* __restrict__ y,
         const double px = x[i], py = y[i], pz = z[i];
         double cx = c.x, cy = c.y, cz = c.z, h = c.w;
         uint64_t key = base < 64 ? (static_cast<uint64_t>(s) << base) : 0ull;
-        if (NB_KEYS_UNROLL) {
-            // a fixed trip count (the deepest key) with the levels past
-            // `levels` masked: the compiler can schedule the whole descent
-#pragma unroll
-            for (int l = 1; l <= 21; ++l) {
-                if (l > levels) break;
-                const bool bx = px > cx, by = py > cy, bz = pz > cz;
-                const uint64_t oct = static_cast<uint64_t>(bx) | (static_cast<uint64_t>(by) << 1) |
-                                     (static_cast<uint64_t>(bz) << 2);
-                key |= oct << (base - 3 * l);
-                const double hs = h * 0.5;
-                cx = cx + (bx ? hs : -hs);
-                cy = cy + (by ? hs : -hs);
-                cz = cz + (bz ? hs : -hs);
-                h = hs;
-            }
-        } else {
-            for (int l = 1; l <= levels; ++l) {
-                const bool bx = px > cx, by = py > cy, bz = pz > cz;
-                const uint64_t oct = static_cast<uint64_t>(bx) | (static_cast<uint64_t>(by) << 1) |
-                                     (static_cast<uint64_t>(bz) << 2);
-                key |= oct << (base - 3 * l);
-                const double hs = h * 0.5;
-                cx = cx + (bx ? hs : -hs);
-                cy = cy + (by ? hs : -hs);
-                cz = cz + (bz ? hs : -hs);
-                h = hs;
-            }
+        for (int l = 1; l <= levels; ++l) {
+            const bool bx = px > cx, by = py > cy, bz = pz > cz;
+            const uint64_t oct = static_cast<uint64_t>(bx) | (static_cast<uint64_t>(by) << 1) |
+                                 (static_cast<uint64_t>(bz) << 2);
+            key |= oct << (base - 3 * l);
+            const double hs = h * 0.5;
+            cx = cx + (bx ? hs : -hs);
+            cy = cy + (by ? hs : -hs);
+            cz = cz + (bz ? hs : -hs);
+            h = hs;
         }
         keys[i] = key;
         idx[i] = static_cast<uint32_t>(i);
