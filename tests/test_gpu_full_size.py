@@ -54,3 +54,27 @@ def test_hernquist_halo_steps_on_device():
     assert np.median(err) <= 1e-3
     assert np.percentile(err, 99) <= 1e-2
     sim.close()
+
+
+def test_ballistic_drift_exact_above_inverse_split():
+    """With G = 0 every body drifts ballistically: after two KDK steps of dt
+    its position is (x + v dt) + v dt in FP64, which the host repeats
+    exactly.  2,200,000 bodies is above the size from which the reorder
+    leaves the inverse permutation (caller index -> position) to a launch of
+    its own, so this checks that launch through every exported lane."""
+    n = 2_200_000
+    rng = np.random.default_rng(11)
+    b = ic.uniform_sphere(n, seed=13)
+    for c in ("vx", "vy", "vz"):
+        b[c] = rng.normal(0.0, 0.1, n)
+    sim = Simulation("accurate", "mixed", theta=0.5, eps=0.01, G=0.0)
+    sim.upload(b)
+    dt = 1e-3
+    sim.steps(dt, 2)
+    st = sim.download()
+    for c, v in (("x", "vx"), ("y", "vy"), ("z", "vz")):
+        expect = (b[c] + b[v] * dt) + b[v] * dt
+        np.testing.assert_array_equal(st[c], expect)
+        np.testing.assert_array_equal(st[v], b[v])
+    assert sim.stats()["device_error"] == 0
+    sim.close()
