@@ -73,15 +73,34 @@ __global__ void __launch_bounds__(kRadix) digit_offsets_kernel(const uint32_t* h
     offsets[p * kRadix + t] = s[t] - hist[p * kRadix + t];
 }
 
-struct SortSmem {
+template <int ITEMS>
+struct SortSmemT {
     uint32_t warp_hist[kWarps][kRadix];
     uint32_t global_delta[kRadix];
     uint32_t warp_total[kWarps];
-    uint64_t keys[kTile];
-    uint32_t vals[kTile];
-    uint32_t peers[kItems][kThreads];   // the count pass's peer masks, reused by the ranking
+    uint64_t keys[kThreads * ITEMS];
+    uint32_t vals[kThreads * ITEMS];
+    uint32_t peers[ITEMS][kThreads];   // the count pass's peer masks, reused by the ranking
     int tile;
 };
+using SortSmem = SortSmemT<kItems>;
+
+// Sorts of at most NB_SORT_SMALL_N pairs (the build's, not the allocation-
+// free entry point's) use tiles of kThreads x NB_SORT_SMALL_ITEMS pairs: a
+// few tiles make such a pass, so its time is about one tile's latency, which
+// shorter tiles cut (16,384 pairs: sort 0.048 -> 0.039 ms).  At 1,048,576
+// pairs the longer look-back chain of twice the tiles costs more than that
+// (0.072 -> 0.079 ms), so larger sorts keep kTile.
+#ifndef NB_SORT_SMALL_N
+#define NB_SORT_SMALL_N 262144
+#endif
+#ifndef NB_SORT_SMALL_ITEMS
+#define NB_SORT_SMALL_ITEMS 8
+#endif
+#ifndef NB_SORT_SMALL_MINB
+#define NB_SORT_SMALL_MINB 4
+#endif
+constexpr int kSmallItems = NB_SORT_SMALL_ITEMS;
 
 // Lanes of the warp whose 8-bit digit equals this lane's: eight ballots,
 // one per digit bit (cheaper than a match-any on this part).  Written as one
@@ -113,12 +132,13 @@ __device__ __forceinline__ uint32_t digit_peers(int dig) {
 // Tile loads into registers: item k of lane l of warp w is pair
 // tile_base + (w * kItems + k) * 32 + l; pairs past n are padding keys that
 // rank after every real key of the tile and are never written out.
+template <int ITEMS>
 __device__ __forceinline__ void load_tile(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-                                          int64_t n, int tile, int w, int lane, uint64_t (&key)[kItems],
-                                          uint32_t (&val)[kItems]) {
-    const int64_t warp_base = static_cast<int64_t>(tile) * kTile + static_cast<int64_t>(w) * kItems * 32;
+                                          int64_t n, int tile, int w, int lane, uint64_t (&key)[ITEMS],
+                                          uint32_t (&val)[ITEMS]) {
+    const int64_t warp_base = static_cast<int64_t>(tile) * (kThreads * ITEMS) + static_cast<int64_t>(w) * ITEMS * 32;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < ITEMS; ++k) {
         const int64_t g = warp_base + k * 32 + lane;
         if (g < n) { key[k] = keys_in[g]; val[k] = vals_in[g]; }
         else { key[k] = ~0ull; val[k] = 0u; }
@@ -129,32 +149,33 @@ __device__ __forceinline__ void load_tile(const uint64_t* __restrict__ keys_in, 
 // tile's pairs sit ranked in shared memory, the block takes its next ticket
 // and loads that tile into the registers the ranking has freed, so the load
 // runs while this tile waits on its look-back and writes itself out.
-__global__ void __launch_bounds__(kThreads, NB_SORT_MINB)
+template <int ITEMS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
 onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint64_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, int64_t n, int shift,
                 uint32_t dmask, const uint32_t* __restrict__ digit_offsets, uint32_t* status, unsigned int* tile_ticket,
                 int* err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SortSmem& S = *reinterpret_cast<SortSmem*>(smem_raw);
+    SortSmemT<ITEMS>& S = *reinterpret_cast<SortSmemT<ITEMS>*>(smem_raw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int ntiles = static_cast<int>((n + kTile - 1) / kTile);
+    const int ntiles = static_cast<int>((n + (kThreads * ITEMS) - 1) / (kThreads * ITEMS));
     if (threadIdx.x == 0) S.tile = static_cast<int>(atomicAdd(tile_ticket, 1u));
     __syncthreads();
     int tile = S.tile;
     // Digits are re-extracted from the keys where needed: holding them (or
     // anything derived from them) across the passes costs more registers.
-    uint64_t key[kItems];
-    uint32_t val[kItems];
+    uint64_t key[ITEMS];
+    uint32_t val[ITEMS];
     if (tile < ntiles) load_tile(keys_in, vals_in, n, tile, w, lane, key, val);
     while (tile < ntiles) {
-        const int64_t tile_base = static_cast<int64_t>(tile) * kTile;
+        const int64_t tile_base = static_cast<int64_t>(tile) * (kThreads * ITEMS);
         for (int i = threadIdx.x; i < kWarps * kRadix; i += kThreads) (&S.warp_hist[0][0])[i] = 0;
         __syncthreads();
         // Per-warp digit counts first (fire-and-forget shared adds by each digit's
         // lowest lane), so the tile's counts are published before the ranking.
         const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
+        for (int k = 0; k < ITEMS; ++k) {
             const int dk = static_cast<int>((key[k] >> shift) & dmask);
             const uint32_t peers = digit_peers(dk);
             S.peers[k][threadIdx.x] = peers;
@@ -197,7 +218,7 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         // precedes item k+1, lanes in order within an item), scattering each key
         // to its local slot as it is ranked.
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
+        for (int k = 0; k < ITEMS; ++k) {
             const int dk = static_cast<int>((key[k] >> shift) & dmask);
             const uint32_t peers = S.peers[k][threadIdx.x];
             const uint32_t base = S.warp_hist[w][dk];
@@ -247,9 +268,9 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
         // global position of local slot i with digit d: global_delta[d] + i
         S.global_delta[d] = digit_offsets[d] + excl - tile_start;
         __syncthreads();
-        const int64_t valid = n - tile_base < kTile ? n - tile_base : kTile;
+        const int64_t valid = n - tile_base < (kThreads * ITEMS) ? n - tile_base : (kThreads * ITEMS);
 #pragma unroll
-        for (int k = 0; k < kItems; ++k) {
+        for (int k = 0; k < ITEMS; ++k) {
             const int i = k * kThreads + threadIdx.x;
             if (i < valid) {
                 const uint64_t kk = S.keys[i];
@@ -267,10 +288,21 @@ onesweep_kernel(const uint64_t* __restrict__ keys_in, const uint32_t* __restrict
 
 }  // namespace
 
+// Pairs per tile of radix_sort_pairs for n pairs.
+static int64_t tile_pairs(int64_t n) {
+    return n <= NB_SORT_SMALL_N ? static_cast<int64_t>(kThreads) * kSmallItems : kTile;
+}
+
+// Scratch words for sorts of up to n pairs with either entry point: hist +
+// offsets (8 x 256 each), tile tickets (8), status (8 x tiles x 256) for the
+// larger of the two tile layouts any such sort can use.
 size_t sort_scratch_words(int64_t n) {
-    const int64_t tiles = (n + kTile - 1) / kTile;
-    // hist + offsets (8 x 256 each), tile tickets (8), status (8 x tiles x 256)
-    return static_cast<size_t>(2 * 8 * kRadix + 8 + 8 * tiles * kRadix);
+    const int64_t small_n = n < NB_SORT_SMALL_N ? n : static_cast<int64_t>(NB_SORT_SMALL_N);
+    const int64_t small_tile = static_cast<int64_t>(kThreads) * kSmallItems;
+    const int64_t small_tiles = small_n > 0 ? (small_n + small_tile - 1) / small_tile : 0;
+    const size_t small = static_cast<size_t>(2 * 8 * kRadix + 8 + 8 * small_tiles * kRadix);
+    const size_t big = static_cast<size_t>(sort_scratch_words_for(n));
+    return small > big ? small : big;
 }
 
 size_t sort_smem_bytes() { return sizeof(SortSmem); }
@@ -281,22 +313,39 @@ size_t sort_smem_bytes() { return sizeof(SortSmem); }
 
 // Blocks of one onesweep pass: every tile's own block, or (persistent) no
 // more than fit on the device at once, each taking tiles until none is left.
+template <int ITEMS, int MINB>
 static unsigned onesweep_grid(int64_t tiles) {
     if (!NB_SORT_PERSISTENT) return static_cast<unsigned>(tiles);
     int dev = 0, sms = 0, per_sm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel, kThreads, sizeof(SortSmem)) !=
-            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<ITEMS, MINB>, kThreads,
+                                                      sizeof(SortSmemT<ITEMS>)) != cudaSuccess ||
         per_sm < 1 || sms < 1)
         return static_cast<unsigned>(tiles);
     const int64_t resident = static_cast<int64_t>(per_sm) * sms;
     return static_cast<unsigned>(tiles < resident ? tiles : resident);
 }
 
+// One pass with tiles of kThreads x ITEMS pairs.
+template <int ITEMS, int MINB>
+static void launch_pass(int64_t n, const uint64_t* ki, const uint32_t* vi, uint64_t* ko, uint32_t* vo, int shift,
+                        uint32_t dmask, const uint32_t* offs, uint32_t* status, unsigned int* ticket, int* err,
+                        cudaStream_t st) {
+    const int64_t tiles = (n + kThreads * ITEMS - 1) / (kThreads * ITEMS);
+    onesweep_kernel<ITEMS, MINB><<<onesweep_grid<ITEMS, MINB>(tiles), kThreads, sizeof(SortSmemT<ITEMS>), st>>>(
+        ki, vi, ko, vo, n, shift, dmask, offs, status, ticket, err);
+}
+
 cudaError_t sort_prepare() {
-    return cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(sizeof(SortSmem)));
+    cudaError_t e = cudaFuncSetAttribute(onesweep_kernel<kItems, NB_SORT_MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(sizeof(SortSmemT<kItems>)));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(onesweep_kernel<kSmallItems, NB_SORT_SMALL_MINB>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sizeof(SortSmemT<kSmallItems>)));
+    return e;
 }
 
 // Sorts (keys, vals) of length n using (alt_keys, alt_vals) as the other
@@ -309,12 +358,14 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
     *in_alt = false;
     if (n <= 1) return cudaSuccess;
     const int passes = (key_bits + 7) / 8;
-    const int64_t tiles = (n + kTile - 1) / kTile;
+    const int64_t tiles = (n + tile_pairs(n) - 1) / tile_pairs(n);
+    const bool small = tile_pairs(n) != kTile;
     uint32_t* hist = scratch;
     uint32_t* offsets = scratch + 8 * kRadix;
     unsigned int* tickets = scratch + 16 * kRadix;
     uint32_t* status = scratch + 16 * kRadix + 8;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * sort_scratch_words(n), st);
+    const size_t words = static_cast<size_t>(2 * 8 * kRadix + 8 + 8 * tiles * kRadix);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * words, st);
     if (e != cudaSuccess) return e;
     int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
     if (hblocks > 1184) hblocks = 1184;
@@ -323,9 +374,13 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, uint64_t* alt_keys,
     uint64_t* src_k = keys; uint32_t* src_v = vals;
     uint64_t* dst_k = alt_keys; uint32_t* dst_v = alt_vals;
     for (int p = 0; p < passes; ++p) {
-        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
-            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
-            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        uint32_t* pst = status + static_cast<int64_t>(p) * tiles * kRadix;
+        if (small)
+            launch_pass<kSmallItems, NB_SORT_SMALL_MINB>(n, src_k, src_v, dst_k, dst_v, 8 * p, pass_mask(key_bits, p),
+                                                         offsets + p * kRadix, pst, tickets + p, err, st);
+        else
+            launch_pass<kItems, NB_SORT_MINB>(n, src_k, src_v, dst_k, dst_v, 8 * p, pass_mask(key_bits, p),
+                                              offsets + p * kRadix, pst, tickets + p, err, st);
         uint64_t* tk = src_k; src_k = dst_k; dst_k = tk;
         uint32_t* tv = src_v; src_v = dst_v; dst_v = tv;
     }
@@ -359,7 +414,7 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
     uint32_t* offsets = scratch + 8 * kRadix;
     unsigned int* tickets = scratch + 16 * kRadix;
     uint32_t* status = scratch + 16 * kRadix + 8;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * sort_scratch_words(n), st);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, sizeof(uint32_t) * static_cast<size_t>(sort_scratch_words_for(n)), st);
     if (e != cudaSuccess) return e;
     int hblocks = static_cast<int>((n + kThreads * 16 - 1) / (kThreads * 16));
     if (hblocks > 1184) hblocks = 1184;
@@ -371,9 +426,9 @@ cudaError_t radix_sort_pairs_to(const uint64_t* keys_in, const uint32_t* vals_in
         const bool to_out = ((passes - 1 - p) & 1) == 0;
         uint64_t* dst_k = to_out ? keys_out : alt_keys;
         uint32_t* dst_v = to_out ? vals_out : alt_vals;
-        onesweep_kernel<<<onesweep_grid(tiles), kThreads, sizeof(SortSmem), st>>>(
-            src_k, src_v, dst_k, dst_v, n, 8 * p, pass_mask(key_bits, p), offsets + p * kRadix,
-            status + static_cast<int64_t>(p) * tiles * kRadix, tickets + p, err);
+        launch_pass<kItems, NB_SORT_MINB>(n, src_k, src_v, dst_k, dst_v, 8 * p, pass_mask(key_bits, p),
+                                          offsets + p * kRadix, status + static_cast<int64_t>(p) * tiles * kRadix,
+                                          tickets + p, err, st);
         src_k = dst_k;
         src_v = dst_v;
     }
