@@ -26,11 +26,17 @@ __global__ void gather_bodies_kernel(Bodies src, Bodies dst, const uint32_t* __r
     if (p >= n) return;
     const uint32_t j = idx[p];
     if (j >= n) { raise_error(err, kErrIndex); return; }
-    dst.x[p] = src.x[j]; dst.y[p] = src.y[j]; dst.z[p] = src.z[j];
-    dst.vx[p] = src.vx[j]; dst.vy[p] = src.vy[j]; dst.vz[p] = src.vz[j];
-    dst.m[p] = src.m[j];
-    dst.type[p] = src.type[j];
+    // every lane's loads before any store: the lanes' pointers may alias as
+    // far as the compiler knows, so interleaved copies would each wait for
+    // the previous store
+    const double x = src.x[j], y = src.y[j], z = src.z[j];
+    const double vx = src.vx[j], vy = src.vy[j], vz = src.vz[j], m = src.m[j];
+    const int type = src.type[j];
     const uint32_t id = src.id[j];
+    dst.x[p] = x; dst.y[p] = y; dst.z[p] = z;
+    dst.vx[p] = vx; dst.vy[p] = vy; dst.vz[p] = vz;
+    dst.m[p] = m;
+    dst.type[p] = type;
     dst.id[p] = id;
     if (inv_here) inv[id] = static_cast<uint32_t>(p);
 }
@@ -48,10 +54,13 @@ __global__ void kick_drift_kernel(Bodies b, int64_t n, const double* __restrict_
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double dt = dts[0], half = dts[1];
-    double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
-    vx += b.ax[i] * half; vy += b.ay[i] * half; vz += b.az[i] * half;
+    // all loads before the first store (the lanes may alias as far as the
+    // compiler knows)
+    const double vx0 = b.vx[i], vy0 = b.vy[i], vz0 = b.vz[i], ax = b.ax[i], ay = b.ay[i], az = b.az[i];
+    const double x0 = b.x[i], y0 = b.y[i], z0 = b.z[i];
+    const double vx = vx0 + ax * half, vy = vy0 + ay * half, vz = vz0 + az * half;
     b.vx[i] = vx; b.vy[i] = vy; b.vz[i] = vz;
-    b.x[i] += vx * dt; b.y[i] += vy * dt; b.z[i] += vz * dt;
+    b.x[i] = x0 + vx * dt; b.y[i] = y0 + vy * dt; b.z[i] = z0 + vz * dt;
 }
 
 // The same kick-drift over a grid-stride loop that also boxes the drifted
@@ -143,7 +152,8 @@ __global__ void kick_kernel(Bodies b, int64_t n, const double* __restrict__ dts,
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double half = dts[1];
-    b.vx[i] += b.ax[i] * half; b.vy[i] += b.ay[i] * half; b.vz[i] += b.az[i] * half;
+    const double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i], ax = b.ax[i], ay = b.ay[i], az = b.az[i];
+    b.vx[i] = vx + ax * half; b.vy[i] = vy + ay * half; b.vz[i] = vz + az * half;
 }
 
 // computeAdaptiveDt (src/dt/adaptive.h:23-52): the largest squared speed is
@@ -303,7 +313,13 @@ __global__ void gather_out_kernel(LaneTable lanes, int count, const uint32_t* __
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t p = inv[i];
-    for (int c = 0; c < count; ++c) out[c * n + i] = lanes.p[c][p];
+    double v[kMaxGatherLanes];
+#pragma unroll
+    for (int c = 0; c < kMaxGatherLanes; ++c)
+        if (c < count) v[c] = lanes.p[c][p];
+#pragma unroll
+    for (int c = 0; c < kMaxGatherLanes; ++c)
+        if (c < count) out[c * n + i] = v[c];
 }
 
 __global__ void ids_to_positions_kernel(const int64_t* __restrict__ ids, const uint32_t* __restrict__ inv, int64_t k,

@@ -253,21 +253,36 @@ __global__ void children_kernel(const uint64_t* __restrict__ keys, const int8_t*
             t.parent[sys] = -1;
             t.level[sys] = 0;
         }
+        // every child's records are loaded before the first store (the tree's
+        // arrays may alias as far as the compiler knows, so loads after a
+        // store would each wait for it), and checked before any store
+        int64_t q2c[8], p2c[8], n2c[8];
+        bool bad = fc + nc > t.cap_node;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int cs = b[c], cnt = b[c + 1] - b[c];
+            q2c[c] = -1; p2c[c] = 0; n2c[c] = 0;
+            if (cnt > leaf_cap && l + 1 < levels) {
+                const int64_t q2 = static_cast<int64_t>(int_base[cs]) + (l + 1 - dlev[cs] - 1);
+                q2c[c] = q2;
+                if (q2 <= q || q2 >= m) bad = true;
+                else { p2c[c] = t.int_packed[q2]; n2c[c] = t.int_packed[q2 + 1]; }
+            }
+        }
+        if (bad) { raise_error(err, kErrIndex); return; }
         int k = 0;
+#pragma unroll
         for (int c = 0; c < 8; ++c) {
             const int cs = b[c], cnt = b[c + 1] - b[c];
             if (cnt == 0) continue;
             const int nid = fc + k++;
             t.parent[nid] = static_cast<int32_t>(q);
             t.level[nid] = static_cast<int8_t>(l + 1);
-            if (nid >= t.cap_node) { raise_error(err, kErrIndex); return; }
-            if (cnt > leaf_cap && l + 1 < levels) {
-                const int64_t q2 = static_cast<int64_t>(int_base[cs]) + (l + 1 - dlev[cs] - 1);
-                if (q2 <= q || q2 >= m) { raise_error(err, kErrIndex); return; }
+            if (q2c[c] >= 0) {
+                const int64_t q2 = q2c[c];
                 t.int_node[q2] = nid;
-                const int64_t p2 = t.int_packed[q2], n2 = t.int_packed[q2 + 1];
-                const int fc2 = nsys + static_cast<int>(p2 & 0xffffffffll);
-                const int nc2 = static_cast<int>((n2 & 0xffffffffll) - (p2 & 0xffffffffll));
+                const int fc2 = nsys + static_cast<int>(p2c[c] & 0xffffffffll);
+                const int nc2 = static_cast<int>((n2c[c] & 0xffffffffll) - (p2c[c] & 0xffffffffll));
                 t.link[nid] = make_int2(fc2, nc2);
                 t.climb[q2] = make_int4(nid, fc2, nc2 | ((l + 1) << 8), cs);
             } else {
@@ -586,12 +601,11 @@ __device__ __forceinline__ void combine_children(const uint64_t* __restrict__ ke
     store_moments(t, nid, p, phalf, prc, P.G, accurate);
 }
 
-// Climb record of internal id q; false (and the index error raised) when it
-// does not describe a node with 1-8 children inside the node array.
-__device__ __forceinline__ bool climb_record(const Tree& t, int64_t nodes, int q, int4* rec, int* err) {
-    *rec = __ldg(t.climb + q);
-    const int nc = rec->z & 0xff;
-    if (rec->x < 0 || rec->x >= nodes || nc < 1 || nc > 8 || rec->y < 0 || static_cast<int64_t>(rec->y) + nc > nodes) {
+// A climb record is valid when it describes a node with 1-8 children inside
+// the node array; false (and the index error raised) otherwise.
+__device__ __forceinline__ bool climb_record_check(int64_t nodes, const int4& rec, int* err) {
+    const int nc = rec.z & 0xff;
+    if (rec.x < 0 || rec.x >= nodes || nc < 1 || nc > 8 || rec.y < 0 || static_cast<int64_t>(rec.y) + nc > nodes) {
         raise_error(err, kErrIndex);
         return false;
     }
@@ -605,12 +619,13 @@ __device__ __forceinline__ void climb_from(int q, bool complete, const uint64_t*
                                           const int32_t* __restrict__ sysid, const double4* __restrict__ cubes,
                                           int base, const Params& P, Tree& t, bool accurate, int64_t nodes,
                                           int64_t ninternal, int* err) {
+    int4 pre = q >= 0 && q < ninternal ? __ldg(t.climb + q) : make_int4(0, 0, 0, 0);
     while (q >= 0) {
         if (q >= ninternal) { raise_error(err, kErrIndex); break; }
-        // the parent's record (written by the child-search pass) and the
-        // arrival both need only q: their round trips overlap
-        int4 rec;
-        const bool ok = climb_record(t, nodes, q, &rec, err);
+        // the parent's record (written by the child-search pass, loaded the
+        // level before) and the arrival both need only q
+        int4 rec = pre;
+        const bool ok = climb_record_check(nodes, rec, err);
         if (!complete) {
             // release this child's moments / acquire the siblings' ones
             const int old = arrive_acq_rel(t.counter + q);
@@ -621,6 +636,8 @@ __device__ __forceinline__ void climb_from(int q, bool complete, const uint64_t*
         }
         complete = false;
         const int next_q = t.parent[rec.x];   // in flight beside the children's loads
+        // the next level's record, loaded before this level's stores
+        if (next_q >= 0 && next_q < ninternal) pre = __ldg(t.climb + next_q);
         combine_children(keys, sysid, cubes, base, P, t, accurate, rec);
         q = next_q;
     }
@@ -663,12 +680,13 @@ upward_leaves_kernel(Bodies bd, int64_t nbodies, const uint64_t* __restrict__ ke
         const int2 lk = t.link[n];
         if (lk.y > 0) continue;
         if (lk.x < 0 || static_cast<int64_t>(lk.x) - lk.y > nbodies) { raise_error(err, kErrIndex); continue; }
-        leaf_moments(bd, keys, sysid, cubes, base, P, t, accurate, n, lk.x, -lk.y);
+        // the parent and its record before the moments' stores
         const int q = t.parent[n];
+        const int4 rec = q >= 0 && q < ninternal ? __ldg(t.climb + q) : make_int4(0, 0, 0, 0);
+        leaf_moments(bd, keys, sysid, cubes, base, P, t, accurate, n, lk.x, -lk.y);
         if (q < 0) continue;
         if (q >= ninternal) { raise_error(err, kErrIndex); continue; }
-        int4 rec;
-        if (!climb_record(t, nodes, q, &rec, err)) continue;
+        if (!climb_record_check(nodes, rec, err)) continue;
         if (atomicAdd(t.counter + q, 1) == (rec.z & 0xff) - 1) {
             t.counter[q] = 0;
             const unsigned long long slot = atomicAdd(reinterpret_cast<unsigned long long*>(t.counts + 4), 1ull);
