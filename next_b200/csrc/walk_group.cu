@@ -337,43 +337,61 @@ __device__ __forceinline__ void eval_batch_packed(const float4* stage, int count
 template <bool QUAD>
 __device__ __forceinline__ void stage_pc_packed(float4* stage, const int* list, int count, const Tree& t, double gcx,
                                                 double gcy, double gcz, float G, int lane) {
+    // both of the lane's entries are loaded before either is stored (1 M
+    // bodies: walk 2.720 -> 2.708 ms against storing each as it arrives)
+    constexpr int kPer = kBatch / 32;
+    float v[kPer][10];
 #pragma unroll
-    for (int e = lane; e < kBatch; e += 32) {
-        float* f = reinterpret_cast<float*>(stage + 5 * (e >> 1)) + (e & 1);
-        float v[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int it = 0; it < kPer; ++it) {
+        const int e = lane + 32 * it;
+#pragma unroll
+        for (int k = 0; k < 10; ++k) v[it][k] = 0.f;
         if (e < count) {
             const int node = list[e];
             const double4 c = t.com[node];
-            v[0] = static_cast<float>(c.x - gcx);
-            v[1] = static_cast<float>(c.y - gcy);
-            v[2] = static_cast<float>(c.z - gcz);
-            v[3] = static_cast<float>(G * c.w);
+            v[it][0] = static_cast<float>(c.x - gcx);
+            v[it][1] = static_cast<float>(c.y - gcy);
+            v[it][2] = static_cast<float>(c.z - gcz);
+            v[it][3] = static_cast<float>(G * c.w);
             if (QUAD) {
                 const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
-                v[4] = q0.x; v[5] = q0.y; v[6] = q0.z; v[7] = q0.w; v[8] = q1.x; v[9] = q1.y;
+                v[it][4] = q0.x; v[it][5] = q0.y; v[it][6] = q0.z; v[it][7] = q0.w; v[it][8] = q1.x; v[it][9] = q1.y;
             }
         }
+    }
 #pragma unroll
-        for (int k = 0; k < 10; ++k) f[2 * k] = v[k];
+    for (int it = 0; it < kPer; ++it) {
+        const int e = lane + 32 * it;
+        float* f = reinterpret_cast<float*>(stage + 5 * (e >> 1)) + (e & 1);
+#pragma unroll
+        for (int k = 0; k < 10; ++k) f[2 * k] = v[it][k];
     }
 }
 
 // Stage up to kBatch bodies of `list` as a packed batch, 2 float4 per pair.
 __device__ __forceinline__ void stage_pp_packed(float4* stage, const int* list, int count, const Bodies& bd,
                                                 double gcx, double gcy, double gcz, float G, int lane) {
+    constexpr int kPer = kBatch / 32;
+    float v[kPer][4];
 #pragma unroll
-    for (int e = lane; e < kBatch; e += 32) {
-        float* f = reinterpret_cast<float*>(stage + 2 * (e >> 1)) + (e & 1);
-        float v[4] = {0, 0, 0, 0};
+    for (int it = 0; it < kPer; ++it) {
+        const int e = lane + 32 * it;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[it][k] = 0.f;
         if (e < count) {
             const int j = list[e];
-            v[0] = static_cast<float>(bd.x[j] - gcx);
-            v[1] = static_cast<float>(bd.y[j] - gcy);
-            v[2] = static_cast<float>(bd.z[j] - gcz);
-            v[3] = static_cast<float>(G * bd.m[j]);
+            v[it][0] = static_cast<float>(bd.x[j] - gcx);
+            v[it][1] = static_cast<float>(bd.y[j] - gcy);
+            v[it][2] = static_cast<float>(bd.z[j] - gcz);
+            v[it][3] = static_cast<float>(G * bd.m[j]);
         }
+    }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) f[2 * k] = v[k];
+    for (int it = 0; it < kPer; ++it) {
+        const int e = lane + 32 * it;
+        float* f = reinterpret_cast<float*>(stage + 2 * (e >> 1)) + (e & 1);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[2 * k] = v[it][k];
     }
 }
 
