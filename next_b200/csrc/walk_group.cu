@@ -553,32 +553,16 @@ struct Fp64Arith {
     __device__ static void pc(unsigned char* stage, const int* list, int count, const Tree& t, const Bodies&,
                               double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
                               int nslices, Acc& A, int lane) {
-        // a lane's entries are all loaded before any is stored, as in the
-        // FP32 staging
         double* st = reinterpret_cast<double*>(stage);
-        constexpr int kPer = kBatch / 32;
-        double v[kPer][10];
+        for (int k = lane; k < count; k += 32) {
+            const int node = list[k];
+            const double4 c = t.com[node];
+            double* e = st + 10 * k;
+            e[0] = c.x - gcx; e[1] = c.y - gcy; e[2] = c.z - gcz; e[3] = G * c.w;
+            if (QUAD) {
+                const double* q = t.quad64 + 8 * static_cast<int64_t>(node);
 #pragma unroll
-        for (int it = 0; it < kPer; ++it) {
-            const int k = lane + 32 * it;
-            if (k < count) {
-                const int node = list[k];
-                const double4 c = t.com[node];
-                v[it][0] = c.x - gcx; v[it][1] = c.y - gcy; v[it][2] = c.z - gcz; v[it][3] = G * c.w;
-                if (QUAD) {
-                    const double* q = t.quad64 + 8 * static_cast<int64_t>(node);
-#pragma unroll
-                    for (int f = 0; f < 6; ++f) v[it][4 + f] = -G * q[f];
-                }
-            }
-        }
-#pragma unroll
-        for (int it = 0; it < kPer; ++it) {
-            const int k = lane + 32 * it;
-            if (k < count) {
-                double* e = st + 10 * k;
-#pragma unroll
-                for (int f = 0; f < (QUAD ? 10 : 4); ++f) e[f] = v[it][f];
+                for (int f = 0; f < 6; ++f) e[4 + f] = -G * q[f];
             }
         }
         __syncwarp();
@@ -589,24 +573,10 @@ struct Fp64Arith {
                               double gcx, double gcy, double gcz, double G, double eps2, bool active, int slice,
                               int nslices, Acc& A, int lane) {
         double* st = reinterpret_cast<double*>(stage);
-        constexpr int kPer = kBatch / 32;
-        double v[kPer][4];
-#pragma unroll
-        for (int it = 0; it < kPer; ++it) {
-            const int k = lane + 32 * it;
-            if (k < count) {
-                const int j = list[k];
-                v[it][0] = bd.x[j] - gcx; v[it][1] = bd.y[j] - gcy; v[it][2] = bd.z[j] - gcz; v[it][3] = G * bd.m[j];
-            }
-        }
-#pragma unroll
-        for (int it = 0; it < kPer; ++it) {
-            const int k = lane + 32 * it;
-            if (k < count) {
-                double* e = st + 4 * k;
-#pragma unroll
-                for (int f = 0; f < 4; ++f) e[f] = v[it][f];
-            }
+        for (int k = lane; k < count; k += 32) {
+            const int j = list[k];
+            double* e = st + 4 * k;
+            e[0] = bd.x[j] - gcx; e[1] = bd.y[j] - gcy; e[2] = bd.z[j] - gcz; e[3] = G * bd.m[j];
         }
         __syncwarp();
         run<4, false>(st, count, eps2, active, slice, nslices, A);
