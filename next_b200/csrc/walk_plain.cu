@@ -94,15 +94,20 @@ walk_plain_kernel(Bodies bd, const int32_t* __restrict__ sysid, int64_t n, Tree 
             }
             const int nd = cur++;
             if (nd < 0 || nd >= nodes) { raise_error(err, kErrIndex); break; }
+            // the node's whole record in one round trip: centre of mass, link
+            // and the 8 moment words (quadrupole, size, critical radius), all
+            // issued before the first test uses any of them
             const double4 c = t.com[nd];
-            if (c.w == 0.0) continue;
             const int2 lk = t.link[nd];
+            const double2* q2 = reinterpret_cast<const double2*>(t.quad64 + 8 * static_cast<int64_t>(nd));
+            const double2 qa = q2[0], qb = q2[1], qc = q2[2], qd = q2[3];
+            const double q64[8] = {qa.x, qa.y, qb.x, qb.y, qc.x, qc.y, qd.x, qd.y};
+            if (c.w == 0.0) continue;
             const bool leaf = lk.y <= 0;
             if (leaf ? (lk.x < 0 || static_cast<int64_t>(lk.x) - lk.y > n) : (sp >= kMaxLevel + 1)) {
                 raise_error(err, leaf ? kErrIndex : kErrStack);
                 break;
             }
-            const double* q64 = t.quad64 + 8 * static_cast<int64_t>(nd);
             if (!ACCURATE) {
                 const int cnt = -lk.y;
                 if (leaf && cnt == 1 && lk.x == i) continue;          // own leaf (octree.h:135)
