@@ -52,6 +52,9 @@ namespace {
 #ifndef NB_WALK_PARTIAL_FIXED
 #define NB_WALK_PARTIAL_FIXED 1
 #endif
+#ifndef NB_WALK_PC_FACTORED
+#define NB_WALK_PC_FACTORED 1
+#endif
 #ifndef NB_WALK_MIN_BLOCKS
 #define NB_WALK_MIN_BLOCKS 5
 #endif
@@ -261,11 +264,21 @@ __device__ __forceinline__ void pc_pair(const float4* e, f2 tx, f2 ty, f2 tz, f2
         const f2 qdy = fma2(qyz, dz, fma2(qyy, dy, mul2(qxy, dx)));
         const f2 qdz = fma2(qzz, dz, fma2(qyz, dy, mul2(qxz, dx)));
         const f2 q = fma2(dz, qdz, fma2(dy, qdy, mul2(dx, qdx)));
-        const f2 cc = mul2(rinv3, fma2(q, mul2(mul2(neg25, rinv2), rinv2), m));
-        const f2 rinv5 = mul2(rinv3, rinv2);
-        s.x = fma2(cc, dx, fma2(rinv5, qdx, s.x));
-        s.y = fma2(cc, dy, fma2(rinv5, qdy, s.y));
-        s.z = fma2(cc, dz, fma2(rinv5, qdz, s.z));
+        if (NB_WALK_PC_FACTORED) {
+            // r2 rinv5 = rinv3, so a = rinv5 (qd + (G m r2 - 2.5 q rinv2) d):
+            // 12 packed operations after q instead of 13
+            const f2 rinv5 = mul2(mul2(rinv2, rinv2), rinv);
+            const f2 k = fma2(mul2(q, rinv2), neg25, mul2(m, r2));
+            s.x = fma2(rinv5, fma2(dx, k, qdx), s.x);
+            s.y = fma2(rinv5, fma2(dy, k, qdy), s.y);
+            s.z = fma2(rinv5, fma2(dz, k, qdz), s.z);
+        } else {
+            const f2 cc = mul2(rinv3, fma2(q, mul2(mul2(neg25, rinv2), rinv2), m));
+            const f2 rinv5 = mul2(rinv3, rinv2);
+            s.x = fma2(cc, dx, fma2(rinv5, qdx, s.x));
+            s.y = fma2(cc, dy, fma2(rinv5, qdy, s.y));
+            s.z = fma2(cc, dz, fma2(rinv5, qdz, s.z));
+        }
     } else {
         const f2 mr3 = mul2(m, rinv3);
         s.x = fma2(mr3, dx, s.x);
