@@ -702,7 +702,9 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
             int total;
             const int off = warp_excl_scan(push, lane, &total);
             if (sp + total > stack_cap) { failed = true; break; }
-            for (int k = 0; k < push; ++k) stack[sp + off + k] = lk.x + k;
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (k < push) stack[sp + off + k] = lk.x + k;
             sp += total;
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
@@ -722,7 +724,11 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
                 const int take = remaining < kPpChunk ? remaining : kPpChunk;
                 int tot;
                 const int o2 = warp_excl_scan(take, lane, &tot);
-                for (int k = 0; k < take; ++k) L.pp[pp_n + o2 + k] = src + k;
+                for (int k0 = 0; k0 < take; k0 += 4) {
+#pragma unroll
+                    for (int k = k0; k < k0 + 4; ++k)
+                        if (k < take) L.pp[pp_n + o2 + k] = src + k;
+                }
                 pp_n += tot;
                 src += take;
                 remaining -= take;
