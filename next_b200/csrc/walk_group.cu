@@ -13,13 +13,14 @@
 //   - accepted cells to the particle-cell (PC) list,
 //   - children of opened cells to the stack,
 //   - bodies of opened leaves to the particle-particle (PP) list,
-// all held in shared memory.  Whenever a list holds 32 entries, the warp
-// stages them (one per lane: FP64 COM/position minus the FP64 group centre,
-// rounded to FP32 -- coordinates relative to the group keep FP32 exact
-// enough near the group) and every lane runs the 32 interactions for its
-// target from shared memory with FP32 FMA and rsqrt.  The 32-term partial
-// is folded into the per-target sum with Kahan compensation.  The FP64
-// arithmetic stages the same entries in FP64 and sums them in FP64.
+// all held in shared memory.  Whenever a list holds kBatch (64) entries, the
+// warp stages them (two per lane: FP64 COM/position minus the FP64 group
+// centre, rounded to FP32 -- coordinates relative to the group keep FP32
+// exact enough near the group) and every lane runs the kBatch interactions
+// for its target from shared memory with packed FP32 FMA and rsqrt.  The
+// batch's partial sum is folded into the per-target sum with Kahan
+// compensation.  The FP64 arithmetic stages the same entries in FP64 and
+// sums them in FP64.
 //
 // Scheduling: persistent blocks (SM count x resident blocks) pull groups
 // from a global atomic work queue.  All waits are warp-synchronous; there
@@ -35,8 +36,11 @@ namespace nb {
 
 namespace {
 
-// Compile-time knobs of the evaluation loop (unroll depth of a full batch and
-// the minimum resident blocks the register allocation must allow).
+// Compile-time knobs of the walk: unroll depth of a full batch, the minimum
+// resident blocks the register allocation must allow, and the traversal's
+// form (fixed-trip list expansion loops, ballot-based scans of the children
+// and body counts, one or two nodes per lane and round).  The defaults are
+// the fastest measured at 1,048,576 bodies.
 #ifndef NB_WALK_UNROLL
 #define NB_WALK_UNROLL 4
 #endif
@@ -51,6 +55,15 @@ namespace {
 #endif
 #ifndef NB_WALK_PARTIAL_FIXED
 #define NB_WALK_PARTIAL_FIXED 1
+#endif
+#ifndef NB_WALK_EXPAND_UNROLLED
+#define NB_WALK_EXPAND_UNROLLED 2
+#endif
+#ifndef NB_WALK_PP_UNROLL
+#define NB_WALK_PP_UNROLL 4
+#endif
+#ifndef NB_WALK_BALLOT_SCAN
+#define NB_WALK_BALLOT_SCAN 2
 #endif
 #ifndef NB_WALK_PC_FACTORED
 #define NB_WALK_PC_FACTORED 1
@@ -70,8 +83,15 @@ constexpr int kWalkGenericUnroll = NB_WALK_GENERIC_UNROLL;
 #endif
 constexpr int kBatch = NB_WALK_BATCH;
 static_assert(kBatch == 32 || kBatch == 64, "evaluation batches of 32 or 64 entries");
-constexpr int kPcCap = kBatch + 32;
+// Nodes popped per lane in each traversal round (1 or 2).
+#ifndef NB_WALK_POP_SLOTS
+#define NB_WALK_POP_SLOTS 1
+#endif
+constexpr int kSlots = NB_WALK_POP_SLOTS;
+static_assert(kSlots == 1 || kSlots == 2, "one or two nodes per lane and round");
+constexpr int kPcCap = kBatch + 32 * kSlots;
 constexpr int kPpChunk = 16;
+static_assert(kPpChunk < 32, "PP chunk counts are scanned as 5-bit values");
 constexpr int kPpCap = kBatch + 32 * kPpChunk;
 
 // Per-warp shared lists; STAGE_BYTES hold one staged evaluation batch.
@@ -82,6 +102,22 @@ struct WarpListsT {
     int pc[kPcCap];
     int pp[kPpCap];
 };
+
+// Exclusive warp scan of values in [0, 2^BITS) from one ballot per bit: the
+// ballots are independent of one another and use no shuffles, so the scan
+// stays off the shared-memory pipe that the evaluation's broadcasts load.
+template <int BITS>
+__device__ __forceinline__ int warp_excl_scan_bits(int v, uint32_t lt, int* total) {
+    int off = 0, tot = 0;
+#pragma unroll
+    for (int b = 0; b < BITS; ++b) {
+        const uint32_t m = __ballot_sync(0xffffffffu, (v >> b) & 1);
+        off += __popc(m & lt) << b;
+        tot += __popc(m) << b;
+    }
+    *total = tot;
+    return off;
+}
 
 __device__ __forceinline__ int warp_excl_scan(int v, int lane, int* total) {
     int inc = v;
@@ -669,42 +705,73 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
         if (lane == 0) { L.gc[0] = gcx; L.gc[1] = gcy; L.gc[2] = gcz; }
         __syncwarp();
         while (sp > 0) {
-            const int nb = sp < 32 ? sp : 32;
+            // pop up to 32 * kSlots nodes: slot k of lane l holds stack[sp + 32 k + l]
+            const int nb = sp < 32 * kSlots ? sp : 32 * kSlots;
             sp -= nb;
-            const int node = lane < nb ? stack[sp + lane] : -1;
-            __syncwarp();
-            bool valid = node >= 0;
-            float4 box = make_float4(0.f, 0.f, 0.f, -1.f);
-            int2 lk = make_int2(0, 0);
-            if (valid) {
-                // index guard: the node, its children or its bodies must lie inside their arrays
-                const bool in_range = static_cast<unsigned>(node) < nnodes32;
-                if (in_range) { box = __ldg(t.box + node); lk = __ldg(t.link + node); }
-                const unsigned end = static_cast<unsigned>(lk.x) + static_cast<unsigned>(lk.y > 0 ? lk.y : -lk.y);
-                const bool bad = !in_range || lk.x < 0 || lk.y > 8 || end > (lk.y > 0 ? nnodes32 : nbodies32);
-                if (bad) raise_error(err, kErrIndex);
-                valid = !bad && box.w >= 0.f;
-            }
-            const float dx = fmaxf(fabsf(box.x - fgx) - hx, 0.f);
-            const float dy = fmaxf(fabsf(box.y - fgy) - hy, 0.f);
-            const float dz = fmaxf(fabsf(box.z - fgz) - hz, 0.f);
-            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            const bool open = valid && d2 < box.w;
-            const bool leaf = lk.y <= 0;
-            const bool accept = valid && !open;
-            const int push = (open && !leaf) ? lk.y : 0;
-            int remaining = (open && leaf) ? -lk.y : 0;
-            // accepted cells -> PC list
-            const uint32_t am = __ballot_sync(0xffffffffu, accept);
-            if (accept) L.pc[pc_n + __popc(am & lt)] = node;
-            pc_n += __popc(am);
-            // children of opened cells -> stack
-            int total;
-            const int off = warp_excl_scan(push, lane, &total);
-            if (sp + total > stack_cap) { failed = true; break; }
+            int node[kSlots];
 #pragma unroll
-            for (int k = 0; k < 8; ++k)
-                if (k < push) stack[sp + off + k] = lk.x + k;
+            for (int k = 0; k < kSlots; ++k) node[k] = lane + 32 * k < nb ? stack[sp + 32 * k + lane] : -1;
+            __syncwarp();
+            float4 box[kSlots];
+            int2 lk[kSlots];
+            bool valid[kSlots];
+#pragma unroll
+            for (int k = 0; k < kSlots; ++k) {
+                valid[k] = node[k] >= 0;
+                box[k] = make_float4(0.f, 0.f, 0.f, -1.f);
+                lk[k] = make_int2(0, 0);
+                // index guard: the node, its children or its bodies must lie inside their arrays
+                if (valid[k] && static_cast<unsigned>(node[k]) < nnodes32) {
+                    box[k] = __ldg(t.box + node[k]);
+                    lk[k] = __ldg(t.link + node[k]);
+                }
+            }
+            int push[kSlots], rem[kSlots];
+#pragma unroll
+            for (int k = 0; k < kSlots; ++k) {
+                if (valid[k]) {
+                    const bool in_range = static_cast<unsigned>(node[k]) < nnodes32;
+                    const unsigned end = static_cast<unsigned>(lk[k].x) +
+                                         static_cast<unsigned>(lk[k].y > 0 ? lk[k].y : -lk[k].y);
+                    const bool bad = !in_range || lk[k].x < 0 || lk[k].y > 8 ||
+                                     end > (lk[k].y > 0 ? nnodes32 : nbodies32);
+                    if (bad) raise_error(err, kErrIndex);
+                    valid[k] = !bad && box[k].w >= 0.f;
+                }
+                const float dx = fmaxf(fabsf(box[k].x - fgx) - hx, 0.f);
+                const float dy = fmaxf(fabsf(box[k].y - fgy) - hy, 0.f);
+                const float dz = fmaxf(fabsf(box[k].z - fgz) - hz, 0.f);
+                const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                const bool open = valid[k] && d2 < box[k].w;
+                const bool leaf = lk[k].y <= 0;
+                const bool accept = valid[k] && !open;
+                push[k] = (open && !leaf) ? lk[k].y : 0;
+                rem[k] = (open && leaf) ? -lk[k].y : 0;
+                // accepted cells -> PC list
+                const uint32_t am = __ballot_sync(0xffffffffu, accept);
+                if (accept) L.pc[pc_n + __popc(am & lt)] = node[k];
+                pc_n += __popc(am);
+            }
+            // children of opened cells -> stack
+            int push_all = 0;
+#pragma unroll
+            for (int k = 0; k < kSlots; ++k) push_all += push[k];
+            int total;
+            const int off = NB_WALK_BALLOT_SCAN ? warp_excl_scan_bits<kSlots == 1 ? 4 : 5>(push_all, lt, &total)
+                                                : warp_excl_scan(push_all, lane, &total);
+            if (sp + total > stack_cap) { failed = true; break; }
+            int o = off;
+#pragma unroll
+            for (int k = 0; k < kSlots; ++k) {
+                if (NB_WALK_EXPAND_UNROLLED) {
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        if (c < push[k]) stack[sp + o + c] = lk[k].x + c;
+                } else {
+                    for (int c = 0; c < push[k]; ++c) stack[sp + o + c] = lk[k].x + c;
+                }
+                o += push[k];
+            }
             sp += total;
             if (sp > max_sp) max_sp = sp;
             __syncwarp();
@@ -712,22 +779,35 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
                 A::pc(L.stage, L.pc, kBatch, t, bd, vld(L.gc[0]), vld(L.gc[1]), vld(L.gc[2]), G, eps2, active, slice,
                       nslices, T, lane);
                 g_pc += kBatch;
-                pc_n -= kBatch;               // < 32 left over
-                const int v = lane < pc_n ? L.pc[kBatch + lane] : 0;
-                __syncwarp();
-                if (lane < pc_n) L.pc[lane] = v;
-                __syncwarp();
+                pc_n -= kBatch;               // < 32 * kSlots left over
+#pragma unroll
+                for (int e0 = 0; e0 < 32 * kSlots; e0 += 32) {
+                    const int v = e0 + lane < pc_n ? L.pc[kBatch + e0 + lane] : 0;
+                    __syncwarp();
+                    if (e0 + lane < pc_n) L.pc[e0 + lane] = v;
+                    __syncwarp();
+                }
             }
-            // bodies of opened leaves -> PP list (in chunks of kPpChunk per lane)
-            int src = lk.x;
-            while (__any_sync(0xffffffffu, remaining > 0)) {
+            // bodies of opened leaves -> PP list (in chunks of kPpChunk per lane;
+            // a lane drains its slot-0 leaf, then its slot-1 leaf)
+            int remaining = rem[0];
+            int src = lk[0].x;
+            int rem2 = kSlots > 1 ? rem[kSlots - 1] : 0;
+            int src2 = kSlots > 1 ? lk[kSlots - 1].x : 0;
+            while (__any_sync(0xffffffffu, remaining > 0 || rem2 > 0)) {
+                if (kSlots > 1 && remaining <= 0) { remaining = rem2; src = src2; rem2 = 0; }
                 const int take = remaining < kPpChunk ? remaining : kPpChunk;
                 int tot;
-                const int o2 = warp_excl_scan(take, lane, &tot);
-                for (int k0 = 0; k0 < take; k0 += 4) {
+                const int o2 = NB_WALK_BALLOT_SCAN > 1 ? warp_excl_scan_bits<5>(take, lt, &tot)
+                                                       : warp_excl_scan(take, lane, &tot);
+                if (NB_WALK_EXPAND_UNROLLED > 1) {
+                    for (int k0 = 0; k0 < take; k0 += NB_WALK_PP_UNROLL) {
 #pragma unroll
-                    for (int k = k0; k < k0 + 4; ++k)
-                        if (k < take) L.pp[pp_n + o2 + k] = src + k;
+                        for (int k = k0; k < k0 + NB_WALK_PP_UNROLL; ++k)
+                            if (k < take) L.pp[pp_n + o2 + k] = src + k;
+                    }
+                } else {
+                    for (int k = 0; k < take; ++k) L.pp[pp_n + o2 + k] = src + k;
                 }
                 pp_n += tot;
                 src += take;
