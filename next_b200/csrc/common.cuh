@@ -65,7 +65,7 @@ struct Tree {
     double4* com;          // FP64 centre of mass and mass
     double* quad64;        // 8 per node: Qxx Qyy Qzz Qxy Qxz Qyz half-width rcrit
     float4* box;           // FP32 COM and rcrit^2 (mixed walk traversal)
-    float4* quad32;        // 2 per node: -G (Qxx Qyy Qzz Qxy) (Qxz Qyz 0 0)
+    float4* quad32;        // 2 per node: -G (Qxx Qyy Qzz Qxy) (Qxz Qyz), G m, 0
     // walk groups
     int4* groups;          // (first body, count, root node, 0)
     int32_t* ready;        // upward pass: internal ids whose children are all leaves

@@ -328,7 +328,7 @@ __device__ __forceinline__ void store_moments(Tree& t, int nid, const Mom& a, do
             make_float4(static_cast<float>(-G * a.q[0]), static_cast<float>(-G * a.q[1]),
                         static_cast<float>(-G * a.q[2]), static_cast<float>(-G * a.q[3]));
         t.quad32[2 * static_cast<int64_t>(nid) + 1] =
-            make_float4(static_cast<float>(-G * a.q[4]), static_cast<float>(-G * a.q[5]), 0.0f, 0.0f);
+            make_float4(static_cast<float>(-G * a.q[4]), static_cast<float>(-G * a.q[5]), static_cast<float>(G * a.m), 0.0f);
     }
 }
 

@@ -65,6 +65,12 @@ namespace {
 #ifndef NB_WALK_BALLOT_SCAN
 #define NB_WALK_BALLOT_SCAN 2
 #endif
+#ifndef NB_WALK_SKIP_EMPTY_PUSH
+#define NB_WALK_SKIP_EMPTY_PUSH 1
+#endif
+#ifndef NB_WALK_GM_FROM_QUAD
+#define NB_WALK_GM_FROM_QUAD 1
+#endif
 #ifndef NB_WALK_PC_FACTORED
 #define NB_WALK_PC_FACTORED 1
 #endif
@@ -401,10 +407,12 @@ __device__ __forceinline__ void stage_pc_packed(float4* stage, const int* list, 
             v[it][0] = static_cast<float>(c.x - gcx);
             v[it][1] = static_cast<float>(c.y - gcy);
             v[it][2] = static_cast<float>(c.z - gcz);
-            v[it][3] = static_cast<float>(G * c.w);
             if (QUAD) {
                 const float4 q0 = t.quad32[2 * node], q1 = t.quad32[2 * node + 1];
+                v[it][3] = NB_WALK_GM_FROM_QUAD ? q1.z : static_cast<float>(G * c.w);
                 v[it][4] = q0.x; v[it][5] = q0.y; v[it][6] = q0.z; v[it][7] = q0.w; v[it][8] = q1.x; v[it][9] = q1.y;
+            } else {
+                v[it][3] = static_cast<float>(G * c.w);
             }
         }
     }
@@ -763,6 +771,7 @@ walk_group_kernel(Bodies bd, int64_t nbodies, Tree t, typename A::Scalar G, type
             int o = off;
 #pragma unroll
             for (int k = 0; k < kSlots; ++k) {
+                if (NB_WALK_SKIP_EMPTY_PUSH && total == 0) break;   // warp-uniform
                 if (NB_WALK_EXPAND_UNROLLED) {
 #pragma unroll
                     for (int c = 0; c < 8; ++c)
