@@ -37,7 +37,7 @@ PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOPS_PP, FLOPS_PC = 20, 56
 # DRAM bytes (read + write) of one walk launch on this workload, from an ncu
 # capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum).
-WALK_DRAM_BYTES = 55.63e6
+WALK_DRAM_BYTES = 56.32e6
 L2_BYTES = 126 * 2 ** 20
 
 
